@@ -1,0 +1,1038 @@
+/* CPU oracle of the SCHISM step: mesh geometry, elevation assembly, JCG, momentum,
+ * vertical velocity, wet/dry levels and nodal velocities (test infrastructure only).
+ *
+ * Plain FP64 restatement of src/kernels/meshdata.cu ("mdc") and meshdata.h ("mdh") in the
+ * order the reference evaluates each expression (compiled with -ffp-contract=off).  State is
+ * kept in reference numbering with per-entity level arrays ([i*nvrt + k]), like the
+ * reference's structs.  Backtracking is in btrack.c, transport in transport.c.
+ * Where the reference relies on thread order (FP64 atomics in the nodal velocities,
+ * mdc:5786-5900; side-boundary linking, mdh:1536-1549) the oracle uses the node's
+ * counter-clockwise element order and side index order.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "oracle.h"
+#include "step_internal.h"
+
+/* ------------------------------------------------------------------ small helpers ---- */
+
+double og_compz(const og_model* m, int i, int k) {
+    /* Node::compZCoord, mdc:1744-1807 (ivcor = 2) */
+    const double eta2 = m->eta2[i], depth = m->depth[i];
+    if (eta2 + depth <= m->h0) return 0.0;                   /* isDry2, mdh:1726 */
+    const double hmod2 = fmin(depth, m->h_s);               /* sigmaTransitionDepth, mdc:1647 */
+    if (k == m->nvrt - 1) return eta2;
+    else if (k == m->nz - 1) return -hmod2;
+    else if (k == m->kb[i]) return -depth;
+    else if (k < m->nz - 1) return m->ztot[k];
+    else {
+        const int ksig = k - (m->nz - 1);
+        if (hmod2 <= m->h_c) return m->sigma[ksig] * (hmod2 + eta2) + eta2;
+        /* the reference asserts when eta2 is below -h_c-(h-h_c)theta_f/sinh(theta_f) */
+        return eta2 * (1.0 + m->sigma[ksig]) + m->h_c * m->sigma[ksig] + (hmod2 - m->h_c) * m->cs[ksig];
+    }
+}
+
+int og_update_kb_value(const og_model* m, int i) {
+    /* Node::updateKb, mdc:1676-1718 (binary search over ztot[0..nz], ztot[nz] = 0) */
+    const double depth = m->depth[i];
+    if (depth <= m->h_s) return m->nz - 1;
+    int kb = -1, L = 0, R = m->nz;
+    while (L <= R) {
+        const int M = (R + L) / 2;
+        if (-depth >= m->ztot[L] && -depth < m->ztot[M]) R = M;
+        else L = M;
+        if (R - L == 1) { kb = L; break; }
+    }
+    return kb;
+}
+
+static inline v2 clampvel(const og_model* m, v2 v) {
+    /* clampVelocity, mdc:192-194 */
+    const double ry = m->rmaxvel * 1.013;
+    return V2(fmin(fmax(v.x, -m->rmaxvel), m->rmaxvel), fmin(fmax(v.y, -ry), ry));
+}
+
+static void tridag(int n, int nc, const double* a, const double* b, const double* c,
+                   const double* rhs, double* u, double* gam) {
+    /* tridag_sch<nc>, mdc:3664-3716 */
+    double bet = b[0];
+    for (int l = 0; l < nc; l++) u[l] = rhs[l] / bet;
+    for (int j = 1; j < n; j++) {
+        gam[j] = c[j - 1] / bet;
+        bet = b[j] - a[j] * gam[j];
+        for (int l = 0; l < nc; l++) u[j * nc + l] = (rhs[j * nc + l] - a[j] * u[(j - 1) * nc + l]) / bet;
+    }
+    for (int j = n - 2; j >= 0; j--)
+        for (int l = 0; l < nc; l++) u[j * nc + l] = u[j * nc + l] - gam[j + 1] * u[(j + 1) * nc + l];
+}
+
+static inline int elem_local(const og_model* m, int e, int i) {
+    for (int j = 0; j < 3; j++) if (m->el[3 * e + j] == i) return j;
+    return -1;
+}
+
+static inline int side_other_elem(const og_model* m, int s, int e) {
+    /* Side::otherElem, mdh:1462-1465 */
+    return (m->isdel[2 * s] == e) ? m->isdel[2 * s + 1] : m->isdel[2 * s];
+}
+
+static inline double side_eta2(const og_model* m, int s) {
+    return 0.5 * (m->eta2[m->isn[2 * s]] + m->eta2[m->isn[2 * s + 1]]);
+}
+static inline double side_depth(const og_model* m, int s) {
+    return 0.5 * (m->depth[m->isn[2 * s]] + m->depth[m->isn[2 * s + 1]]);
+}
+static inline double side_htot2(const og_model* m, int s) { return side_eta2(m, s) + side_depth(m, s); }
+static inline double side_Dz(const og_model* m, int s, int k) {
+    return m->zc[s * m->nvrt + k] - m->zc[s * m->nvrt + k - 1];
+}
+static inline double side_Cd(const og_model* m, int s) {
+    if (!m->sdry[s]) return 0.5 * (m->Cd[m->isn[2 * s]] + m->Cd[m->isn[2 * s + 1]]);
+    return 0.0;
+}
+static inline v2 side_tau(const og_model* m, int s) {
+    const int a = m->isn[2 * s], b = m->isn[2 * s + 1];
+    return V2S(V2ADD(V2(m->tau[2 * a], m->tau[2 * a + 1]), V2(m->tau[2 * b], m->tau[2 * b + 1])), 0.5);
+}
+static inline int side_is2d(const og_model* m, int s) { return m->kbs[s] == m->nvrt - 2; }
+
+/* ------------------------------------------------------------------ creation ---- */
+
+static void* xc(size_t n, size_t sz) { void* p = calloc(n ? n : 1, sz); return p; }
+
+og_model* og_model_create(const og_input* in, int* status) {
+    og_model* m = (og_model*)xc(1, sizeof(og_model));
+    *status = 0;
+    m->np = in->np; m->ne = in->ne; m->nvrt = in->nvrt; m->ntr = in->ntr;
+    m->nope = in->nope; m->nland = in->nland; m->nbfr = in->nbfr;
+    m->dt = in->dt; m->thetai = in->thetai; m->h0 = in->h0; m->dtb_min = in->dtb_min;
+    m->dtb_max = in->dtb_max; m->velmin = in->velmin_btrack; m->rmaxvel = in->rmaxvel;
+    m->dfv0 = in->dfv0; m->coricoef = in->coricoef; m->rho0 = in->rho0; m->grav = in->grav;
+    m->dramp = in->dramp; m->ihhat = in->ihhat;
+    m->nz = in->nz; m->h_s = in->h_s; m->h_c = in->h_c; m->theta_b = in->theta_b; m->theta_f = in->theta_f;
+    const int np = m->np, ne = m->ne, nvrt = m->nvrt, ntr = m->ntr;
+    m->ztot = (double*)xc(nvrt + 1, sizeof(double));
+    for (int k = 0; k < in->nz; k++) m->ztot[k] = in->ztot[k];
+    const int nsig = nvrt - in->nz + 1;
+    m->sigma = (double*)xc(nvrt, sizeof(double));
+    m->cs = (double*)xc(nvrt, sizeof(double));
+    for (int k = 0; k < nsig; k++) {
+        const double s = in->sigma[k], tb = in->theta_b, tf = in->theta_f;
+        m->sigma[k] = s;
+        /* read_and_process_grid.cpp:1492-1494 */
+        m->cs[k] = (1.0 - tb) * sinh(tf * s) / sinh(tf) +
+                   tb * (tanh(tf * (s + 0.5)) - tanh(tf * 0.5)) / 2.0 / tanh(tf * 0.5);
+    }
+
+    /* connectivity exactly as readHGrid (oracle/grid.c) */
+    int32_t* el4 = (int32_t*)xc((size_t)ne * 4, sizeof(int32_t));
+    int32_t* i34 = (int32_t*)xc(ne, sizeof(int32_t));
+    for (int e = 0; e < ne; e++) {
+        for (int j = 0; j < 3; j++) el4[4 * e + j] = in->elnode[3 * e + j];
+        el4[4 * e + 3] = -1; i34[e] = 3;
+    }
+    m->isbnd = (int32_t*)xc(np, sizeof(int32_t));
+    og_grid_isbnd(np, in->nope, in->open_start, in->open_nodes, in->nland, in->land_start,
+                  in->land_nodes, m->isbnd);
+    m->nne_s = (int32_t*)xc(np + 1, sizeof(int32_t));
+    m->nne = (int32_t*)xc((size_t)4 * ne + 1, sizeof(int32_t));
+    m->nnp_s = (int32_t*)xc(np + 1, sizeof(int32_t));
+    m->nnp = (int32_t*)xc((size_t)4 * ne + np + 1, sizeof(int32_t));
+    int32_t* ic3 = (int32_t*)xc((size_t)4 * ne, sizeof(int32_t));
+    int32_t* es4 = (int32_t*)xc((size_t)4 * ne, sizeof(int32_t));
+    int32_t* isdel = (int32_t*)xc((size_t)8 * ne + 8, sizeof(int32_t));
+    int32_t* isn = (int32_t*)xc((size_t)8 * ne + 8, sizeof(int32_t));
+    int32_t ns = 0;
+    int rc = og_grid_build(np, ne, el4, i34, m->isbnd, m->nne_s, m->nne, m->nnp_s, m->nnp, ic3, es4,
+                           isdel, isn, &ns);
+    if (rc != 0) { *status = rc; free(el4); free(i34); free(ic3); free(es4); free(isdel); free(isn); return m; }
+    m->ns = ns;
+    m->el = (int32_t*)xc((size_t)3 * ne, sizeof(int32_t));
+    m->es = (int32_t*)xc((size_t)3 * ne, sizeof(int32_t));
+    for (int e = 0; e < ne; e++)
+        for (int j = 0; j < 3; j++) { m->el[3 * e + j] = el4[4 * e + j]; m->es[3 * e + j] = es4[4 * e + j]; }
+    m->isdel = (int32_t*)xc((size_t)2 * ns, sizeof(int32_t));
+    m->isn = (int32_t*)xc((size_t)2 * ns, sizeof(int32_t));
+    memcpy(m->isdel, isdel, sizeof(int32_t) * 2 * ns);
+    memcpy(m->isn, isn, sizeof(int32_t) * 2 * ns);
+    free(el4); free(i34); free(ic3); free(es4); free(isdel); free(isn);
+
+    /* node arrays */
+    m->x = (double*)xc(np, 8); m->y = (double*)xc(np, 8); m->depth = (double*)xc(np, 8);
+    m->drag = (double*)xc(np, 8); m->Cd = (double*)xc(np, 8); m->grav2 = (double*)xc(np, 8);
+    m->tau = (double*)xc((size_t)2 * np, 8);
+    memcpy(m->x, in->x, 8 * (size_t)np); memcpy(m->y, in->y, 8 * (size_t)np);
+    memcpy(m->depth, in->depth, 8 * (size_t)np); memcpy(m->drag, in->drag, 8 * (size_t)np);
+    memcpy(m->tau, in->tau, 16 * (size_t)np);
+    m->eta1 = (double*)xc(np, 8); m->eta2 = (double*)xc(np, 8);
+    m->qel = (double*)xc(np, 8); m->mX = (double*)xc(np, 8); m->elbc = (double*)xc(np, 8);
+    m->kb = (int32_t*)xc(np, 4); m->ndry = (uint8_t*)xc(np, 1); m->nwas = (uint8_t*)xc(np, 1);
+    m->z = (double*)xc((size_t)np * nvrt, 8);
+    m->u2 = (v2*)xc((size_t)np * nvrt, sizeof(v2));
+    m->w2 = (double*)xc((size_t)np * nvrt, 8);
+    m->tr = (double*)xc((size_t)np * nvrt * (ntr ? ntr : 1), 8);
+    m->tr_init = (double*)xc((size_t)np * nvrt * (ntr ? ntr : 1), 8);
+    for (int t = 0; t < ntr; t++)
+        for (int k = 0; k < nvrt; k++)
+            for (int i = 0; i < np; i++)
+                m->tr_init[((size_t)i * nvrt + k) * ntr + t] = in->tr_init[((size_t)t * nvrt + k) * np + i];
+    m->ess = (uint8_t*)xc(np, 1);
+    m->nbfr_emo = (double*)xc((size_t)np * (m->nbfr ? m->nbfr : 1), 8);
+    m->nbfr_efa = (double*)xc((size_t)np * (m->nbfr ? m->nbfr : 1), 8);
+    m->sb1 = (int32_t*)xc(np, 4); m->sb2 = (int32_t*)xc(np, 4);
+    m->x0 = (double*)xc(np, 8); m->x1 = (double*)xc(np, 8); m->x2 = (double*)xc(np, 8);
+    m->xs = (double*)xc(np, 8);
+    m->amig = (double*)xc(m->nbfr, 8); m->ff = (double*)xc(m->nbfr, 8); m->face = (double*)xc(m->nbfr, 8);
+    for (int f = 0; f < m->nbfr; f++) { m->amig[f] = in->amig[f]; m->ff[f] = in->ff[f]; m->face[f] = in->face[f]; }
+    m->seg_iettype = (int32_t*)xc(m->nope, 4);
+    for (int k = 0; k < m->nope; k++) m->seg_iettype[k] = in->iettype[k];
+    m->open_start = (int32_t*)xc(m->nope + 1, 4);
+    m->open_nodes = (int32_t*)xc(in->nope ? in->open_start[in->nope] : 1, 4);
+    m->land_start = (int32_t*)xc(m->nland + 1, 4);
+    m->land_nodes = (int32_t*)xc(in->nland ? in->land_start[in->nland] : 1, 4);
+    memcpy(m->open_start, in->open_start, 4 * (size_t)(m->nope + 1));
+    if (m->nope) memcpy(m->open_nodes, in->open_nodes, 4 * (size_t)in->open_start[m->nope]);
+    memcpy(m->land_start, in->land_start, 4 * (size_t)(m->nland + 1));
+    if (m->nland) memcpy(m->land_nodes, in->land_nodes, 4 * (size_t)in->land_start[m->nland]);
+    /* populateBoundaryNodes, mdc:2483-2533: the last matching (segment, position) wins */
+    for (int k = 0; k < m->nope; k++)
+        for (int j = in->open_start[k]; j < in->open_start[k + 1]; j++) {
+            const int i = in->open_nodes[j];
+            m->ess[i] = (in->iettype[k] != 0);
+            for (int f = 0; f < m->nbfr; f++) {
+                m->nbfr_emo[(size_t)i * m->nbfr + f] = in->emo[(size_t)j * m->nbfr + f];
+                m->nbfr_efa[(size_t)i * m->nbfr + f] = in->efa[(size_t)j * m->nbfr + f];
+            }
+        }
+
+    /* side arrays */
+    const int nss = ns;
+    m->len = (double*)xc(nss, 8); m->snx = (double*)xc(nss, 8); m->sny = (double*)xc(nss, 8);
+    m->scx = (double*)xc(nss, 8); m->scy = (double*)xc(nss, 8); m->cori = (double*)xc(nss, 8);
+    m->kbs = (int32_t*)xc(nss, 4); m->sdry = (uint8_t*)xc(nss, 1);
+    m->sbt = (int8_t*)xc(nss, 1);
+    m->zc = (double*)xc((size_t)nss * nvrt, 8);
+    m->su2 = (v2*)xc((size_t)nss * nvrt, sizeof(v2));
+    m->btu = (v2*)xc((size_t)nss * nvrt, sizeof(v2));
+    m->btel = (int32_t*)xc((size_t)nss * nvrt, 4);
+    m->U = (v2*)xc(nss, sizeof(v2));
+    m->hhat = (double*)xc(nss, 8); m->chi = (double*)xc(nss, 8); m->chi2 = (double*)xc(nss, 8);
+    m->gE1 = (v2*)xc(nss, sizeof(v2)); m->gE2 = (v2*)xc(nss, sizeof(v2));
+    m->Qh = (double*)xc((size_t)nss * nvrt, 8);
+
+    /* element arrays */
+    m->area = (double*)xc(ne, 8); m->edepth = (double*)xc(ne, 8);
+    m->gphi = (v2*)xc((size_t)3 * ne, sizeof(v2)); m->ssign = (double*)xc((size_t)3 * ne, 8);
+    m->kbe = (int32_t*)xc(ne, 4); m->edry = (uint8_t*)xc(ne, 1);
+    m->ez = (double*)xc((size_t)ne * nvrt, 8);
+    m->ew = (double*)xc((size_t)ne * nvrt, 8);
+    m->Qv = (double*)xc((size_t)ne * nvrt, 8);
+    m->etr = (double*)xc((size_t)ne * nvrt * (ntr ? ntr : 1), 8);
+    m->prev = (double*)xc((size_t)ne * nvrt * (ntr ? ntr : 1), 8);
+    m->inflow = (double*)xc((size_t)ne * nvrt, 8);
+    m->maxDt = (double*)xc(ne, 8);
+    m->ghat = (v2*)xc(ne, sizeof(v2));
+
+    /* CSR pattern */
+    m->nnz = m->nnp_s[np] + np;
+    m->indptr = (int32_t*)xc(np + 1, 4);
+    m->indices = (int32_t*)xc(m->nnz, 4);
+    m->data = (double*)xc(m->nnz, 8);
+    m->slot = (int32_t*)xc(m->nnp_s[np] + 1, 4);
+    m->dslot = (int32_t*)xc(np, 4);
+    m->jr = (double*)xc(np, 8); m->jz = (double*)xc(np, 8); m->jp = (double*)xc(np, 8);
+    m->jq = (double*)xc(np, 8); m->jinvD = (double*)xc(np, 8); m->jb = (double*)xc(np, 8);
+    return m;
+}
+
+void og_model_free(og_model* m) {
+    if (!m) return;
+    void* ptrs[] = {m->ztot, m->sigma, m->cs, m->isbnd, m->nne_s, m->nne, m->nnp_s, m->nnp, m->el, m->es,
+                    m->isdel, m->isn, m->x, m->y, m->depth, m->drag, m->Cd, m->grav2, m->tau, m->eta1,
+                    m->eta2, m->qel, m->mX, m->elbc, m->kb, m->ndry, m->nwas, m->z, m->u2, m->w2, m->tr,
+                    m->tr_init, m->ess, m->nbfr_emo, m->nbfr_efa, m->sb1, m->sb2, m->x0, m->x1, m->x2,
+                    m->xs, m->amig, m->ff, m->face, m->seg_iettype, m->open_start, m->open_nodes,
+                    m->land_start, m->land_nodes, m->len, m->snx, m->sny, m->scx, m->scy, m->cori,
+                    m->kbs, m->sdry, m->sbt, m->zc, m->su2, m->btu, m->btel, m->U, m->hhat, m->chi,
+                    m->chi2, m->gE1, m->gE2, m->Qh, m->area, m->edepth, m->gphi, m->ssign, m->kbe,
+                    m->edry, m->ez, m->ew, m->Qv, m->etr, m->prev, m->inflow, m->maxDt, m->ghat,
+                    m->indptr, m->indices, m->data, m->slot, m->dslot, m->jr, m->jz, m->jp, m->jq,
+                    m->jinvD, m->jb};
+    for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
+    free(m);
+}
+
+int og_model_sizes(const og_model* m, int* np, int* ne, int* ns, int* nnz) {
+    *np = m->np; *ne = m->ne; *ns = m->ns; *nnz = m->nnz;
+    return 0;
+}
+
+/* ------------------------------------------------------------------ initialisation ---- */
+
+static int seg_pair(const int32_t* start, const int32_t* nodes, int nseg, int a, int b) {
+    /* findSideBoundaryType, mdc:1860-1900: consecutive pair (a,b) in some segment */
+    for (int k = 0; k < nseg; k++)
+        for (int j = start[k]; j < start[k + 1] - 1; j++) {
+            const int b1 = nodes[j], b2 = nodes[j + 1];
+            if ((b1 == a && b2 == b) || (b1 == b && b2 == a)) return k;
+        }
+    return -1;
+}
+
+int og_model_init(og_model* m) {
+    const int np = m->np, ne = m->ne, ns = m->ns, nvrt = m->nvrt, ntr = m->ntr;
+    /* populateNodes, mdc:1903-2092 (ics = 1, nchi = 0, itur = 0) */
+    for (int i = 0; i < np; i++) {
+        m->Cd[i] = m->drag[i];
+        m->grav2[i] = m->grav;                            /* scaleGravity, iloadtide = 0 */
+        for (int k = 0; k < nvrt; k++) {
+            m->z[(size_t)i * nvrt + k] = 0.0;
+            for (int t = 0; t < ntr; t++)
+                m->tr[((size_t)i * nvrt + k) * ntr + t] = m->tr_init[((size_t)i * nvrt + k) * ntr + t];
+        }
+        m->sb1[i] = -1; m->sb2[i] = -1;
+        m->kb[i] = og_update_kb_value(m, i);
+    }
+    /* populateNodes2, mdc:2094-2141: CSR rows sorted by column, diagonal included */
+    for (int i = 0; i < np; i++) {
+        const int s0 = m->nnp_s[i], nn = m->nnp_s[i + 1] - s0;
+        const int rowStart = s0 + i;
+        m->indptr[i] = rowStart;
+        for (int a = 0; a < nn; a++) {
+            const int col = m->nnp[s0 + a];
+            int idx = (i < col) ? 1 : 0;
+            for (int b = 0; b < nn; b++) if (m->nnp[s0 + b] < col) idx++;
+            m->slot[s0 + a] = idx;
+        }
+        int d = 0;
+        for (int b = 0; b < nn; b++) if (m->nnp[s0 + b] < i) d++;
+        m->dslot[i] = d;
+        m->indices[rowStart + d] = i;
+        for (int a = 0; a < nn; a++) m->indices[rowStart + m->slot[s0 + a]] = m->nnp[s0 + a];
+    }
+    m->indptr[np] = m->nnz;
+    /* populateSides, mdc:2146-2347 */
+    for (int s = 0; s < ns; s++) {
+        const int a = m->isn[2 * s], b = m->isn[2 * s + 1];
+        m->scx[s] = 0.5 * (m->x[a] + m->x[b]);
+        m->scy[s] = 0.5 * (m->y[a] + m->y[b]);
+        v2 n = V2(-(m->y[a] - m->y[b]), (m->x[a] - m->x[b]));
+        const double ln = sqrt(n.x * n.x + n.y * n.y);
+        m->snx[s] = n.x / ln; m->sny[s] = n.y / ln;
+        const double dx = m->x[b] - m->x[a], dy = m->y[b] - m->y[a], dz = 0.0 - 0.0;
+        m->len[s] = sqrt(dx * dx + dy * dy + dz * dz);
+        m->cori[s] = m->coricoef;                        /* ncor = 0 */
+        m->sbt[s] = 0;
+        if (m->isbnd[a] != -1 && m->isbnd[b] != -1) {
+            if (seg_pair(m->land_start, m->land_nodes, m->nland, a, b) >= 0) m->sbt[s] = 1;
+            else if (seg_pair(m->open_start, m->open_nodes, m->nope, a, b) >= 0) m->sbt[s] = 2;
+            if (m->sbt[s]) {
+                /* linkSideBoundary, mdh:1536-1549: open nodes only, first free slot */
+                const int nn[2] = {a, b};
+                for (int q = 0; q < 2; q++) {
+                    const int i = nn[q];
+                    if (m->isbnd[i] < 0) continue;
+                    if (m->sb1[i] < 0) m->sb1[i] = s;
+                    else if (m->sb2[i] < 0) m->sb2[i] = s;
+                }
+            }
+        }
+        for (int k = 0; k < nvrt; k++) m->zc[(size_t)s * nvrt + k] = 0.0;
+    }
+    /* populateElements, mdc:2350-2480 */
+    for (int e = 0; e < ne; e++) {
+        const int* nd = &m->el[3 * e];
+        double cx = 0.0, cy = 0.0, dep = 1e10;
+        for (int j = 0; j < 3; j++) {
+            cx += m->x[nd[j]] / 3; cy += m->y[nd[j]] / 3;
+            dep = fmin(dep, m->depth[nd[j]]);
+        }
+        (void)cx; (void)cy;
+        m->edepth[e] = dep;
+        const double x0 = m->x[nd[0]], y0 = m->y[nd[0]], x1 = m->x[nd[1]], y1 = m->y[nd[1]];
+        const double x2 = m->x[nd[2]], y2 = m->y[nd[2]];
+        const double area = 0.5 * ((x0 - x2) * (y1 - y2) - (x1 - x2) * (y0 - y2));
+        m->area[e] = area;
+        for (int j = 0; j < 3; j++) {
+            const int s = m->es[3 * e + j];
+            m->ssign[3 * e + j] = (m->isdel[2 * s] == e) ? 1.0 : -1.0;
+            const int p2 = nd[(j + 1) % 3], p3 = nd[(j + 2) % 3];
+            m->gphi[3 * e + j] = V2((m->y[p2] - m->y[p3]) / (2 * area), (m->x[p3] - m->x[p2]) / (2 * area));
+        }
+        /* initial element tracers: node levels k and k-1 averaged, level 0 = level 1 */
+        const double inv = 1.0 / (2.0 * 3);
+        for (int k = 1; k < nvrt; k++)
+            for (int t = 0; t < ntr; t++) {
+                double sum = 0.0;
+                for (int j = 0; j < 3; j++)
+                    sum += m->tr_init[((size_t)nd[j] * nvrt + k) * ntr + t] +
+                           m->tr_init[((size_t)nd[j] * nvrt + k - 1) * ntr + t];
+                m->etr[((size_t)e * nvrt + k) * ntr + t] = inv * sum;
+            }
+        for (int t = 0; t < ntr; t++)
+            m->etr[((size_t)e * nvrt + 0) * ntr + t] = m->etr[((size_t)e * nvrt + 1) * ntr + t];
+    }
+    /* schism_init.py:81-91: cold-start levels (it = iths = 0) */
+    og_levels(m, 0);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ forcing ---- */
+
+void og_begin_step(og_model* m, int it) {
+    /* schism_step.py:103-179 restricted to the supported physics */
+    const double time = it * m->dt;
+    m->time = time;
+    /* computeTimeRamps, mdh:2036-2077 */
+    m->ramp = (m->dramp > 0.0) ? tanh(2.0 * time / 86400.0 / m->dramp) : 1.0;
+    for (int i = 0; i < m->np; i++) {
+        m->grav2[i] = m->grav;       /* scaleGravity, mdc:3945-3972, iloadtide = 0 */
+        m->Cd[i] = m->drag[i];       /* computeBottomDragCd, mdc:1810-1812 (nchi = 0) */
+    }
+}
+
+/* ------------------------------------------------------------------ elevation ---- */
+
+void og_prepare_elevation(og_model* m, double time) {
+    const int np = m->np, ne = m->ne, ns = m->ns, nvrt = m->nvrt;
+    const double dt = m->dt;
+    /* computeElevationBoundaryConditions, mdc:4276-4339 */
+    for (int i = 0; i < np; i++) {
+        if (m->isbnd[i] < 0) continue;
+        const int iettype = m->seg_iettype[m->isbnd[i]];
+        const double eic = 0.0;
+        const double r_eic = (1.0 - m->ramp) * eic;
+        const double r_eth = m->ramp * 0.0;
+        double r_eta1_bar = 0.0;
+        if (iettype == 3 || iettype == 5) {
+            for (int f = 0; f < m->nbfr; f++) {
+                const double efa = m->nbfr_efa[(size_t)i * m->nbfr + f];
+                const double emo = m->nbfr_emo[(size_t)i * m->nbfr + f];
+                const int ncyc = (int)(m->amig[f] * time / (2.0 * M_PI));
+                const double arg = m->amig[f] * time - (2.0 * M_PI) * ncyc + m->face[f] - efa;
+                r_eta1_bar += m->ramp * m->ff[f] * emo * cos(arg);
+            }
+        }
+        if (iettype == 1 || iettype == 2 || iettype == 4) m->elbc[i] = r_eic + r_eth;
+        else if (iettype == 3) m->elbc[i] = r_eic + r_eta1_bar;
+        else if (iettype == 5) m->elbc[i] = r_eic + r_eta1_bar + r_eth;
+    }
+    /* computeVerticallyIntegratedVelocity, mdc:4459-4476 */
+    for (int s = 0; s < ns; s++) {
+        m->U[s] = V2(0.0, 0.0);
+        if (m->sdry[s]) continue;
+        for (int k = m->kbs[s]; k < nvrt - 1; k++) {
+            const v2 uc = V2S(V2ADD(m->su2[(size_t)s * nvrt + k], m->su2[(size_t)s * nvrt + k + 1]), 0.5);
+            m->U[s] = V2ADD(m->U[s], V2S(uc, side_Dz(m, s, k + 1)));
+        }
+    }
+    /* computeVegetationAndDragParameters, mdc:4615-4725 (iveg = 0) */
+    for (int s = 0; s < ns; s++) {
+        m->hhat[s] = 0.0; m->chi2[s] = 0.0; m->chi[s] = 0.0;
+        if (m->sdry[s]) continue;
+        const double htot = side_htot2(m, s);
+        const int kb = m->kbs[s];
+        const v2 b = m->btu[(size_t)s * nvrt + kb + 1];
+        const double vmag1 = sqrt(b.x * b.x + b.y * b.y);
+        m->chi2[s] = side_Cd(m, s) * vmag1;
+        m->chi[s] = m->chi2[s];
+        if (side_is2d(m, s)) {
+            const double fricH = htot + m->chi2[s] * dt;
+            m->hhat[s] = htot * htot / fricH;
+        } else {
+            m->hhat[s] = htot - m->chi[s] * dt;
+            if (m->ihhat == 1) m->hhat[s] = fmax(0.0, m->hhat[s]);
+        }
+    }
+    /* computeElemAverageGhat, mdc:6183-6424 (ics = 1, iveg = 0, ibc = 1, nuGradU = 0,
+     * no atmospheric pressure or tidal potential gradients) */
+    for (int e = 0; e < ne; e++) {
+        m->ghat[e] = V2(0.0, 0.0);
+        if (m->edry[e]) continue;
+        double av_cff1 = 0.0, av_cff2 = 0.0;
+        const int i34 = 3;
+        v2 g = V2(0.0, 0.0);
+        for (int j = 0; j < i34; j++) {
+            const int s = m->es[3 * e + j];
+            const double chi = m->chi[s];
+            const double htot = side_htot2(m, s);
+            double cff1, cff2;
+            if (side_is2d(m, s)) { cff1 = m->hhat[s] / htot; cff2 = 0.0; }
+            else { cff1 = 1.0; cff2 = 1.0; }
+            av_cff1 += cff1 / i34;
+            av_cff2 += cff2 / i34;
+            v2 Ustar = V2(0.0, 0.0);
+            if (side_is2d(m, s)) {
+                Ustar = V2ADD(Ustar, V2S(m->btu[(size_t)s * nvrt + nvrt - 1], side_Dz(m, s, nvrt - 1)));
+            } else {
+                for (int k = m->kbs[s] + 1; k < nvrt; k++) {
+                    const v2 w2 = V2S(V2DIV(V2ADD(m->btu[(size_t)s * nvrt + k], m->btu[(size_t)s * nvrt + k - 1]), 2.0),
+                                      side_Dz(m, s, k));
+                    Ustar = V2ADD(Ustar, w2);
+                }
+            }
+            g = V2ADD(g, V2S(Ustar, cff1));
+            const v2 tau = side_tau(m, s);
+            const v2 ubstar = m->btu[(size_t)s * nvrt + m->kbs[s] + 1];
+            g = V2SUB(g, V2ADD(V2S(ubstar, chi * dt * cff2), V2S(tau, dt * cff1)));
+            const double cor = m->cori[s];
+            const v2 F = V2S(m->U[s], cor);
+            const v2 fb = V2S(m->su2[(size_t)s * nvrt + m->kbs[s] + 1], cor);
+            g = V2ADD(g, V2SUB(V2S(F, cff1 * dt), V2S(fb, cff2 * chi * dt * dt)));
+        }
+        g = V2S(g, 1.0 / i34);
+        (void)av_cff1; (void)av_cff2;   /* they multiply the (zero) pressure/potential force */
+        m->ghat[e] = g;
+    }
+}
+
+static void add_to_row(og_model* m, int i, int col, double value) {
+    /* Node::addToSparseMatrix, mdh:1771-1786 */
+    if (col == i) { m->data[m->indptr[i] + m->dslot[i]] += value; return; }
+    const int s0 = m->nnp_s[i], s1 = m->nnp_s[i + 1];
+    for (int a = s0; a < s1; a++)
+        if (m->nnp[a] == col) { m->data[m->indptr[i] + m->slot[a]] += value; return; }
+}
+
+void og_assemble(og_model* m, double time) {
+    /* setupCoefficientMatrixAndRHS, mdc:3182-3474 (triangles, imm = 0, ifltype = 0) */
+    (void)time;
+    const double dt = m->dt, th = m->thetai;
+    for (int i = 0; i < m->np; i++) {
+        for (int a = m->indptr[i]; a < m->indptr[i + 1]; a++) m->data[a] = 0.0;
+        double qel = 0.0;
+        for (int q = m->nne_s[i]; q < m->nne_s[i + 1]; q++) {
+            const int e = m->nne[q];
+            const int* nd = &m->el[3 * e];
+            const int* sd = &m->es[3 * e];
+            const double grav3 = (m->grav2[nd[0]] + m->grav2[nd[1]] + m->grav2[nd[2]] + 0.0) / 3;
+            const double hhatb = (m->hhat[sd[0]] + m->hhat[sd[1]] + m->hhat[sd[2]] + 0.0) / 3;
+            const int id1 = elem_local(m, e, i);
+            const double area = m->area[e];
+            const v2 U = V2DIV(V2ADD(V2ADD(V2ADD(m->U[sd[0]], m->U[sd[1]]), m->U[sd[2]]), V2(0.0, 0.0)), 3);
+            const v2 gp1 = m->gphi[3 * e + id1];
+            const double I41 = V2DOT(gp1, U);
+            const double I42 = V2DOT(gp1, m->ghat[e]);
+            qel += dt * area * ((1 - th) * I41 + th * I42);
+            const double fricCoeff = grav3 * th * (1.0 - th) * dt * dt * hhatb;
+            const int id2 = (id1 + 1) % 3, id3 = (id1 + 2) % 3;
+            const int n2 = nd[id2], n3 = nd[id3];
+            const v2 p0 = V2(m->x[nd[id1]], m->y[nd[id1]]);
+            const v2 p1 = V2(m->x[n2], m->y[n2]);
+            const v2 p2 = V2(m->x[n3], m->y[n3]);
+            const double ipp_ii = (1.0 / 6.0) * area, ipp_ij = (1.0 / 12.0) * area, ipp_ik = (1.0 / 12.0) * area;
+            const double igpgp_ii = ((1.0 / 4.0) / area) * V2DOT(V2SUB(p2, p1), V2SUB(p2, p1));
+            const double igpgp_ij = ((1.0 / 4.0) / area) * V2DOT(V2SUB(p2, p1), V2SUB(p0, p2));
+            const double igpgp_ik = -igpgp_ii - igpgp_ij;
+            const double c = grav3 * th * th * dt * dt * hhatb;
+            add_to_row(m, i, i, ipp_ii + c * igpgp_ii);
+            add_to_row(m, i, n2, ipp_ij + c * igpgp_ij);
+            add_to_row(m, i, n3, ipp_ik + c * igpgp_ik);
+            const double wet = m->edry[e] ? 0.0 : 1.0;
+            for (int l = 0; l < 3; l++) {
+                const int nl = nd[l];
+                const double ipp = ((id1 == l) ? (2.0 / 12.0) : (1.0 / 12.0)) * area;
+                const double igpgp = area * V2DOT(m->gphi[3 * e + id1], m->gphi[3 * e + l]);
+                qel += (m->eta2[nl] + 0.0) * ipp - m->eta2[nl] * fricCoeff * igpgp * wet;
+            }
+            qel += (dt / 3) * 0.0;                                  /* vsource = 0 */
+        }
+        /* boundary integrals of open-boundary nodes: only I_5 survives for ifltype = 0 */
+        if (m->isbnd[i] >= 0) {
+            const int sbl[2] = {m->sb1[i], m->sb2[i]};
+            for (int l = 0; l < 2; l++) {
+                const int s = sbl[l];
+                if (s < 0) continue;
+                if (!m->sdry[s]) {
+                    const double Unbar = m->U[s].x * m->snx[s] + m->U[s].y * m->sny[s];
+                    qel -= 0.5 * (1.0 - th) * dt * m->len[s] * Unbar;
+                }
+            }
+        }
+        m->qel[i] = qel;
+    }
+}
+
+void og_essential_bc(og_model* m) {
+    /* rollUpElevation, mdc:3538-3544, then setEssentialBC, mdc:4400-4446 */
+    for (int i = 0; i < m->np; i++) m->eta1[i] = m->eta2[i];
+    for (int i = 0; i < m->np; i++) {
+        if (m->isbnd[i] >= 0 && m->ess[i]) {
+            for (int a = m->indptr[i]; a < m->indptr[i + 1]; a++) m->data[a] = 0.0;
+            m->data[m->indptr[i] + m->dslot[i]] = 1.0;
+            m->mX[i] = m->elbc[i];
+            m->qel[i] = m->elbc[i];
+        } else {
+            for (int a = m->nnp_s[i]; a < m->nnp_s[i + 1]; a++) {
+                const int nb = m->nnp[a];
+                if (m->isbnd[nb] >= 0 && m->ess[nb]) {
+                    const int idx = m->indptr[i] + m->slot[a];
+                    m->qel[i] -= m->data[idx] * m->elbc[nb];
+                    m->data[idx] = 0.0;
+                }
+            }
+        }
+    }
+}
+
+static void spmv(const og_model* m, const double* v, double* out) {
+    for (int i = 0; i < m->np; i++) {
+        double s = 0.0;
+        for (int a = m->indptr[i]; a < m->indptr[i + 1]; a++) s += m->data[a] * v[m->indices[a]];
+        out[i] = s;
+    }
+}
+
+int og_jcg_solve(og_model* m, double rtol, int maxiter, int check_every, double* relres) {
+    /* PCGSolverMultiGPU.solve, pcg_solver.py:1075-1124, with the compiled loop's scalar rules
+     * (pcg_solver.py:208-276): beta = 0 on the first pass or when rz_old = 0, alpha = 0 when
+     * p.q = 0, convergence r.r <= (rtol |b|)^2 tested every check_every iterations. */
+    const int n = m->np;
+    double* b = m->jb; double* x = m->xs; double* r = m->jr; double* z = m->jz;
+    double* p = m->jp; double* q = m->jq; double* invD = m->jinvD;
+    double bb = 0.0;
+    for (int i = 0; i < n; i++) { b[i] = m->qel[i]; bb += b[i] * b[i]; }
+    for (int i = 0; i < n; i++) invD[i] = 1.0 / m->data[m->indptr[i] + m->dslot[i]];
+    const double atol = rtol * sqrt(bb);
+    int iters = 0;
+    if (atol == 0.0) {
+        for (int i = 0; i < n; i++) x[i] = 0.0;
+    } else {
+        for (int i = 0; i < n; i++) { x[i] = 3.0 * m->x0[i] - 3.0 * m->x1[i] + m->x2[i]; p[i] = 0.0; }
+        spmv(m, x, q);
+        for (int i = 0; i < n; i++) r[i] = b[i] - q[i];
+        const double atol2 = atol * atol;
+        double rz = 0.0, rr = 0.0;
+        for (int i = 0; i < n; i++) { z[i] = invD[i] * r[i]; rr += r[i] * r[i]; rz += r[i] * z[i]; }
+        double rho = rz;
+        iters = maxiter;
+        for (int it = 0; it < maxiter; it++) {
+            const double beta = (it == 0 || rho == 0.0) ? 0.0 : m->jrz_new / rho;
+            if (it > 0) rho = m->jrz_new;
+            for (int i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+            spmv(m, p, q);
+            double pq = 0.0;
+            for (int i = 0; i < n; i++) pq += p[i] * q[i];
+            const double alpha = (pq != 0.0) ? rho / pq : 0.0;
+            rr = 0.0; rz = 0.0;
+            for (int i = 0; i < n; i++) {
+                x[i] += alpha * p[i];
+                r[i] = r[i] - alpha * q[i];
+                z[i] = invD[i] * r[i];
+                rr += r[i] * r[i]; rz += r[i] * z[i];
+            }
+            m->jrz_new = rz;
+            if ((it + 1) % check_every == 0 || it == maxiter - 1) {
+                if (rr <= atol2) { iters = it + 1; break; }
+            }
+        }
+    }
+    /* scatterXToMesh + rollHistory, pcg_solver.py:941-947 */
+    for (int i = 0; i < n; i++) {
+        m->mX[i] = x[i];
+        m->x2[i] = m->x1[i]; m->x1[i] = m->x0[i]; m->x0[i] = x[i];
+    }
+    if (relres) {
+        spmv(m, x, q);
+        double rn = 0.0;
+        for (int i = 0; i < n; i++) { const double d = b[i] - q[i]; rn += d * d; }
+        *relres = bb > 0 ? sqrt(rn) / sqrt(bb) : sqrt(rn);
+    }
+    m->cnt[0] = iters;
+    return iters;
+}
+
+void og_update_elevation(og_model* m) {
+    /* updateElevation, mdc:4449-4456: eta2 = solution; kb refresh for wet nodes */
+    for (int i = 0; i < m->np; i++) {
+        m->eta2[i] = m->mX[i];
+        if (!m->ndry[i]) m->kb[i] = og_update_kb_value(m, i);
+    }
+}
+
+/* ------------------------------------------------------------------ momentum ---- */
+
+static v2 side_grad(const og_model* m, int s, const double* f, int which) {
+    /* Side::grad2, mdc:1330-1373; which = 1: wet elements (isDry), 2: wet by eta2 (isDry2) */
+    v2 g = V2(0.0, 0.0);
+    int count = 0;
+    for (int l = 0; l < 2; l++) {
+        const int e = m->isdel[2 * s + l];
+        if (e < 0) continue;
+        int ok;
+        if (which == 1) ok = !m->edry[e];
+        else {
+            const int* nd = &m->el[3 * e];
+            ok = !((m->eta2[nd[0]] + m->depth[nd[0]] <= m->h0) || (m->eta2[nd[1]] + m->depth[nd[1]] <= m->h0) ||
+                   (m->eta2[nd[2]] + m->depth[nd[2]] <= m->h0));
+        }
+        if (!ok) continue;
+        const int* nd = &m->el[3 * e];
+        const v2* gp = &m->gphi[3 * e];
+        const double gx = f[nd[0]] * gp[0].x + f[nd[1]] * gp[1].x + f[nd[2]] * gp[2].x;
+        const double gy = f[nd[0]] * gp[0].y + f[nd[1]] * gp[1].y + f[nd[2]] * gp[2].y;
+        g = V2ADD(g, V2(gx, gy));
+        count++;
+    }
+    if (count > 0) g = V2S(g, 1.0 / count);
+    return g;
+}
+
+void og_momentum(og_model* m, double time) {
+    (void)time;
+    const int ns = m->ns, nvrt = m->nvrt;
+    const double dt = m->dt, th = m->thetai;
+    /* computeHorGradientAtSide, mdc:5045-5073 (pressure and tidal potential are zero) */
+    for (int s = 0; s < ns; s++) {
+        if (m->sdry[s]) continue;
+        m->gE1[s] = side_grad(m, s, m->eta1, 1);
+        m->gE2[s] = side_grad(m, s, m->eta2, 2);
+    }
+    double* alow = (double*)malloc(sizeof(double) * nvrt);
+    double* cupp = (double*)malloc(sizeof(double) * nvrt);
+    double* bdia = (double*)malloc(sizeof(double) * nvrt);
+    double* rrhs = (double*)malloc(sizeof(double) * 2 * nvrt);
+    double* soln = (double*)malloc(sizeof(double) * 2 * nvrt);
+    double* gam = (double*)malloc(sizeof(double) * nvrt);
+    /* solveMomentumEquations, mdc:5076-5354 */
+    for (int s = 0; s < ns; s++) {
+        v2* u2 = &m->su2[(size_t)s * nvrt];
+        const v2* btu = &m->btu[(size_t)s * nvrt];
+        if (m->sdry[s]) {
+            for (int k = 0; k < nvrt; k++) u2[k] = V2(0.0, 0.0);
+            continue;
+        }
+        const int kb = m->kbs[s];
+        const int a = m->isn[2 * s], b = m->isn[2 * s + 1];
+        const double grav3 = 0.5 * (m->grav2[a] + m->grav2[b]);
+        const double cor = m->cori[s];
+        if (side_is2d(m, s)) {
+            const double htot = m->zc[(size_t)s * nvrt + nvrt - 1] - m->zc[(size_t)s * nvrt + kb];
+            const double hhat = m->hhat[s];
+            const v2 tau2 = side_tau(m, s);
+            const v2 corT = V2S(V2(u2[nvrt - 1].y, -u2[nvrt - 1].x), cor);
+            const v2 inner = V2SUB(V2ADD(corT, V2DIV(tau2, htot)),
+                                   V2S(V2ADD(V2S(m->gE1[s], 1 - th), V2S(m->gE2[s], th)), grav3));
+            const v2 hat_gam = V2ADD(btu[nvrt - 1], V2S(inner, dt));
+            const v2 vel = clampvel(m, V2DIV(V2S(hat_gam, hhat), htot));
+            for (int k = 0; k < nvrt; k++) u2[k] = vel;
+        } else {
+            for (int k = kb + 1; k < nvrt; k++) {
+                const int kin = k - (kb + 1);
+                alow[kin] = 0.0; cupp[kin] = 0.0; bdia[kin] = 0.0;
+                const double cff1 = 1.0;
+                if (k < nvrt - 1) {
+                    const double dzz = side_Dz(m, s, k + 1);
+                    const double dfz = 0.5 * (m->dfv0 + m->dfv0);
+                    const double tmp = dt * dfz / dzz;
+                    cupp[kin] += cff1 * dzz / 6.0 - tmp;
+                    bdia[kin] += cff1 * dzz / 3.0 + tmp;
+                }
+                if (k > kb + 1) {
+                    const double dzz = side_Dz(m, s, k);
+                    const double dfz = 0.5 * (m->dfv0 + m->dfv0);
+                    const double tmp = dt * dfz / dzz;
+                    alow[kin] += cff1 * dzz / 6.0 - tmp;
+                    bdia[kin] += cff1 * dzz / 3.0 + tmp;
+                } else {
+                    bdia[kin] += dt * m->chi2[s];
+                }
+            }
+            const v2 grad2D = V2S(V2ADD(V2S(m->gE2[s], th), V2S(m->gE1[s], 1.0 - th)), grav3);
+            for (int k = kb + 1; k < nvrt; k++) {
+                const int kin = k - kb - 1;
+                const double dz_0 = side_Dz(m, s, k);
+                const double dz_1 = (k < nvrt - 1) ? side_Dz(m, s, k + 1) : 0.0;
+                double dz = 0.0;
+                dz += dz_1;
+                if (k > kb + 1) dz += dz_0;
+                v2 rh = V2S(grad2D, -(0.5 * dz) * dt);
+                if (k < nvrt - 1) {
+                    const v2 uu = V2ADD(V2S(u2[k], 2.0), u2[k + 1]);
+                    const v2 cterm = V2S(V2(uu.y, -uu.x), cor);
+                    const v2 inner = V2ADD(V2ADD(V2S(btu[k], 2.0), btu[k + 1]), V2S(cterm, dt));
+                    rh = V2ADD(rh, V2S(inner, dz_1 / 6.0));
+                } else {
+                    rh = V2ADD(rh, V2S(side_tau(m, s), dt));
+                }
+                if (k > kb + 1) {
+                    const v2 uu = V2ADD(V2S(u2[k], 2.0), u2[k - 1]);
+                    const v2 cterm = V2S(V2(uu.y, -uu.x), cor);
+                    const v2 inner = V2ADD(V2ADD(V2S(btu[k], 2.0), btu[k - 1]), V2S(cterm, dt));
+                    rh = V2ADD(rh, V2S(inner, dz_0 / 6.0));
+                }
+                rrhs[2 * kin] = rh.x; rrhs[2 * kin + 1] = rh.y;
+            }
+            tridag(nvrt - kb - 1, 2, alow, bdia, cupp, rrhs, soln, gam);
+            for (int k = kb + 1; k < nvrt; k++) {
+                const int kin = k - kb - 1;
+                u2[k] = clampvel(m, V2(soln[2 * kin], soln[2 * kin + 1]));
+            }
+        }
+        if (side_Cd(m, s) == 0.0) u2[kb] = u2[kb + 1];
+        else if (!side_is2d(m, s)) u2[kb] = V2(0.0, 0.0);
+        for (int k = 0; k < kb; k++) u2[k] = V2(0.0, 0.0);
+    }
+    free(alow); free(cupp); free(bdia); free(rrhs); free(soln); free(gam);
+    /* applyMomentumBC, mdc:5357-5454: free slip on land sides (islip = 0) */
+    for (int s = 0; s < ns; s++) {
+        if (m->sbt[s] != 1) continue;
+        v2* u2 = &m->su2[(size_t)s * nvrt];
+        const v2 t = V2(-m->sny[s], m->snx[s]);
+        const v2 n = V2(m->snx[s], m->sny[s]);
+        for (int k = m->kbs[s]; k < nvrt; k++) {
+            const double vnorm = 0.0;
+            const double vtan = V2DOT(u2[k], t);
+            u2[k] = V2SUB(V2S(t, vtan), V2S(n, vnorm));
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ vertical velocity ---- */
+
+static void elem_normal(const og_model* m, int e, int k, double* nx, double* ny, double* nz, double* area3D) {
+    /* Element::n, mdc:558-633 (triangles, ics = 1) */
+    const int* nd = &m->el[3 * e];
+    const int nvrt = m->nvrt;
+    const int k0 = k > m->kb[nd[0]] ? k : m->kb[nd[0]];
+    const int k1 = k > m->kb[nd[1]] ? k : m->kb[nd[1]];
+    const int k2 = k > m->kb[nd[2]] ? k : m->kb[nd[2]];
+    const double x0 = m->x[nd[0]], y0 = m->y[nd[0]], z0 = m->z[(size_t)nd[0] * nvrt + k0];
+    const double x1 = m->x[nd[1]], y1 = m->y[nd[1]], z1 = m->z[(size_t)nd[1] * nvrt + k1];
+    const double x2 = m->x[nd[2]], y2 = m->y[nd[2]], z2 = m->z[(size_t)nd[2] * nvrt + k2];
+    const double n20x = x2 - x0, n20y = y2 - y0, n20z = z2 - z0;
+    const double n10x = x1 - x0, n10y = y1 - y0, n10z = z1 - z0;
+    const double ax = n10y * n20z - n20y * n10z;
+    const double ay = n20x * n10z - n10x * n20z;
+    const double az = 2.0 * m->area[e];
+    const double len = sqrt(ax * ax + ay * ay + az * az);
+    *area3D = 0.5 * len;
+    const double inv = 1.0 / len;
+    *nx = ax * inv; *ny = ay * inv; *nz = az * inv;
+}
+
+void og_vertical_velocity(og_model* m) {
+    /* computeVerticalVelocity, mdc:5978-6103 (imm = 0, ics = 1) */
+    const int nvrt = m->nvrt;
+    for (int e = 0; e < m->ne; e++) {
+        double* w = &m->ew[(size_t)e * nvrt];
+        double* Qv = &m->Qv[(size_t)e * nvrt];
+        for (int l = 0; l < nvrt; l++) w[l] = 0.0;
+        if (m->edry[e]) continue;
+        const int kb = m->kbe[e];
+        const int* nd = &m->el[3 * e];
+        const int* sd = &m->es[3 * e];
+        const v2* gp = &m->gphi[3 * e];
+        const double ghx = m->depth[nd[0]] * gp[0].x + m->depth[nd[1]] * gp[1].x + m->depth[nd[2]] * gp[2].x;
+        const double ghy = m->depth[nd[0]] * gp[0].y + m->depth[nd[1]] * gp[1].y + m->depth[nd[2]] * gp[2].y;
+        v2 ub = V2(0.0, 0.0);
+        for (int j = 0; j < 3; j++) ub = V2ADD(ub, m->su2[(size_t)sd[j] * nvrt + m->kbs[sd[j]]]);
+        ub = V2DIV(V2ADD(ub, V2(0.0, 0.0)), 3);
+        const double bottomW = -(ghx * ub.x + ghy * ub.y);
+        w[kb] = 0.0 + bottomW;
+        double bottomFlux = 0.0;
+        Qv[kb] = 0.0;
+        for (int l = kb; l < nvrt - 1; l++) {
+            double tnx, tny, tnz, tA;
+            elem_normal(m, e, l + 1, &tnx, &tny, &tnz, &tA);
+            double sideFlux = 0.0;
+            for (int j = 0; j < 3; j++) {
+                const int s = sd[j];
+                const int kbs = m->kbs[s];
+                const v2 ut = m->su2[(size_t)s * nvrt + (l + 1 > kbs ? l + 1 : kbs)];
+                const v2 ubt = m->su2[(size_t)s * nvrt + (l > kbs ? l : kbs)];
+                const v2 u2c = V2S(V2ADD(ut, ubt), 0.5);
+                const int ka = (l + 1 > kbs) ? l + 1 : kbs, kc = (l > kbs) ? l : kbs;
+                const double sideArea = m->len[s] * (m->zc[(size_t)s * nvrt + ka] - m->zc[(size_t)s * nvrt + kc]);
+                const double sign = m->ssign[3 * e + j];
+                sideFlux += sign * (u2c.x * m->snx[s] + u2c.y * m->sny[s]) * sideArea;
+            }
+            v2 um = V2(0.0, 0.0);
+            for (int j = 0; j < 3; j++) {
+                const int s = sd[j];
+                const int kk = (l + 1 > m->kbs[s]) ? l + 1 : m->kbs[s];
+                um = V2ADD(um, m->su2[(size_t)s * nvrt + kk]);
+            }
+            um = V2DIV(V2ADD(um, V2(0.0, 0.0)), 3);
+            const double topFlux = -sideFlux - bottomFlux;
+            Qv[l + 1] = topFlux;
+            const double topH = (um.x * tnx + um.y * tny) * tA;
+            const double topV = topFlux - topH;
+            w[l + 1] = topV / (tnz * tA);
+            bottomFlux = -topFlux;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ levels / wet-dry ---- */
+
+void og_levels(og_model* m, int it) {
+    const int np = m->np, ne = m->ne, ns = m->ns, nvrt = m->nvrt, ntr = m->ntr;
+    /* ul0UpdateZCoords, mdc:5521-5547 */
+    for (int i = 0; i < np; i++) {
+        m->kb[i] = og_update_kb_value(m, i);
+        for (int k = m->kb[i]; k < nvrt; k++) m->z[(size_t)i * nvrt + k] = og_compz(m, i, k);
+        m->nwas[i] = m->ndry[i];
+        m->ndry[i] = 1;
+    }
+    /* ul0ComputeDryElements, mdc:5550-5593 */
+    for (int e = 0; e < ne; e++) {
+        const int* nd = &m->el[3 * e];
+        int dry = 0;
+        for (int j = 0; j < 3; j++) if (m->eta2[nd[j]] + m->depth[nd[j]] <= m->h0) dry = 1;
+        m->edry[e] = (uint8_t)dry;
+        m->kbe[e] = 0;
+        if (dry) continue;
+        const int k1 = m->kb[nd[0]], k2 = m->kb[nd[1]], k3 = m->kb[nd[2]];
+        int kb = k1 < k2 ? k1 : k2; kb = kb < k3 ? kb : k3;
+        m->kbe[e] = kb;
+        for (int k = kb; k < nvrt; k++) {
+            double zz = m->z[(size_t)nd[0] * nvrt + (k > k1 ? k : k1)] + m->z[(size_t)nd[1] * nvrt + (k > k2 ? k : k2)] +
+                        m->z[(size_t)nd[2] * nvrt + (k > k3 ? k : k3)];
+            zz /= 3;
+            m->ez[(size_t)e * nvrt + k] = zz;
+        }
+    }
+    /* ul0ComputeDryNodes, mdc:5596-5613 */
+    for (int i = 0; i < np; i++) {
+        m->ndry[i] = 1;
+        for (int q = m->nne_s[i]; q < m->nne_s[i + 1]; q++)
+            if (!m->edry[m->nne[q]]) { m->ndry[i] = 0; break; }
+    }
+    /* ul0UpdateRewettedNodes, mdc:5616-5676 (all tracers averaged, not only T and S) */
+    if (it != 0) {
+        for (int i = 0; i < np; i++) {
+            if (!(!m->ndry[i] && m->nwas[i])) continue;
+            for (int k = 0; k < nvrt; k++) {
+                double ux = 0.0, uy = 0.0, uw = 0.0;
+                double ts[64];
+                for (int t = 0; t < ntr && t < 64; t++) ts[t] = 0.0;
+                int icount = 0;
+                for (int a = m->nnp_s[i]; a < m->nnp_s[i + 1]; a++) {
+                    const int nb = m->nnp[a];
+                    if (m->nwas[nb]) continue;
+                    icount++;
+                    ux += m->u2[(size_t)nb * nvrt + k].x; uy += m->u2[(size_t)nb * nvrt + k].y;
+                    uw += m->w2[(size_t)nb * nvrt + k];
+                    for (int t = 0; t < ntr && t < 64; t++) ts[t] += m->tr[((size_t)nb * nvrt + k) * ntr + t];
+                }
+                if (icount > 0) {
+                    const double inv = 1.0 / icount;
+                    m->u2[(size_t)i * nvrt + k] = V2(inv * ux, inv * uy);
+                    m->w2[(size_t)i * nvrt + k] = inv * uw;
+                    for (int t = 0; t < ntr && t < 64; t++) m->tr[((size_t)i * nvrt + k) * ntr + t] = inv * ts[t];
+                } else {
+                    m->u2[(size_t)i * nvrt + k] = V2(0.0, 0.0);
+                    m->w2[(size_t)i * nvrt + k] = 0.0;
+                }
+            }
+        }
+    }
+    /* ul0UpdateSides, mdc:5679-5745 */
+    for (int s = 0; s < ns; s++) {
+        const int e0 = m->isdel[2 * s], e1 = m->isdel[2 * s + 1];
+        const int wet = !m->edry[e0] || (e1 >= 0 && !m->edry[e1]);
+        const int a = m->isn[2 * s], b = m->isn[2 * s + 1];
+        const int kb1 = m->kb[a], kb2 = m->kb[b];
+        m->kbs[s] = 0;
+        if (!wet) continue;
+        m->kbs[s] = kb1 < kb2 ? kb1 : kb2;
+        for (int k = 0; k < m->kbs[s]; k++) m->zc[(size_t)s * nvrt + k] = 0.0;
+        for (int k = m->kbs[s]; k < nvrt; k++) {
+            m->zc[(size_t)s * nvrt + k] = 0.5 * (m->z[(size_t)a * nvrt + (k > kb1 ? k : kb1)] +
+                                                  m->z[(size_t)b * nvrt + (k > kb2 ? k : kb2)]);
+            if (it != 0 && m->sdry[s]) {
+                v2 ut = V2(0.0, 0.0);
+                int icount = 0;
+                for (int j = 0; j < 2; j++) {
+                    const int e = m->isdel[2 * s + j];
+                    if (e < 0) continue;
+                    for (int jj = 0; jj < 3; jj++) {
+                        const int ss = m->es[3 * e + jj];
+                        if (m->sdry[ss]) continue;
+                        icount++;
+                        ut = V2ADD(ut, m->su2[(size_t)ss * nvrt + k]);
+                    }
+                }
+                m->su2[(size_t)s * nvrt + k] = (icount > 0) ? V2DIV(ut, icount) : V2(0.0, 0.0);
+            }
+        }
+    }
+    /* ul0UpdateSides2, mdc:5748-5762 */
+    for (int s = 0; s < ns; s++) {
+        const int e0 = m->isdel[2 * s], e1 = m->isdel[2 * s + 1];
+        const int wet = !m->edry[e0] || (e1 >= 0 && !m->edry[e1]);
+        m->sdry[s] = (uint8_t)!wet;
+    }
+}
+
+/* ------------------------------------------------------------------ nodal velocities ---- */
+
+void og_nodal_velocities(og_model* m) {
+    /* zeroNodalVelocities .. computeNodalHorizontalVelocities2, mdc:5765-5929, as a
+     * node-centred gather in counter-clockwise element order (indvel <= 0, triangles) */
+    const int nvrt = m->nvrt;
+    for (int i = 0; i < m->np; i++) {
+        double* w2 = &m->w2[(size_t)i * nvrt];
+        v2* u2 = &m->u2[(size_t)i * nvrt];
+        for (int k = 0; k < nvrt; k++) { w2[k] = 0.0; u2[k] = V2(0.0, 0.0); }
+        double asum = 0.0;
+        const int kbn = m->kb[i];
+        for (int q = m->nne_s[i]; q < m->nne_s[i + 1]; q++) {
+            const int e = m->nne[q];
+            for (int k = kbn; k < nvrt; k++) w2[k] += m->ew[(size_t)e * nvrt + k] * m->area[e];
+            asum += m->area[e];
+        }
+        const double inv = 1.0 / asum;
+        for (int k = kbn; k < nvrt; k++) w2[k] = inv * w2[k];
+        int count = 0;
+        for (int q = m->nne_s[i]; q < m->nne_s[i + 1]; q++) {
+            const int e = m->nne[q];
+            if (m->edry[e] || m->ndry[i]) continue;
+            const int j = elem_local(m, e, i);
+            const int s1 = m->es[3 * e + j], s2 = m->es[3 * e + (j + 1) % 3], s3 = m->es[3 * e + (j + 2) % 3];
+            count++;
+            for (int k = m->kbe[e]; k < nvrt; k++) {
+                const v2 u = clampvel(m, V2SUB(V2ADD(m->su2[(size_t)s2 * nvrt + k], m->su2[(size_t)s3 * nvrt + k]),
+                                               m->su2[(size_t)s1 * nvrt + k]));
+                u2[k] = V2ADD(u2[k], u);
+            }
+        }
+        if (count == 0) {
+            for (int k = 0; k < nvrt; k++) u2[k] = V2(0.0, 0.0);
+        } else {
+            for (int k = 0; k < kbn; k++) u2[k] = V2(0.0, 0.0);
+            for (int k = kbn; k < nvrt; k++) u2[k] = V2S(u2[k], 1.0 / count);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ whole step ---- */
+
+int og_step(og_model* m, int it) {
+    /* schism_step.py:95-334 */
+    og_begin_step(m, it);
+    const double time = m->time;
+    og_btrack(m);
+    og_prepare_elevation(m, time);
+    og_assemble(m, time);
+    og_essential_bc(m);
+    const int iters = og_jcg_solve(m, m->rtol, m->maxiter, m->check_every, NULL);
+    og_update_elevation(m);
+    og_momentum(m, time);
+    og_vertical_velocity(m);
+    og_transport(m, m->dt);
+    og_levels(m, it);
+    og_nodal_velocities(m);
+    return iters;
+}
+
+void og_counters(const og_model* m, int64_t* out4) {
+    for (int i = 0; i < 4; i++) out4[i] = m->cnt[i];
+}
+
+void og_set_solver(og_model* m, double rtol, int maxiter, int check_every) {
+    m->rtol = rtol; m->maxiter = maxiter; m->check_every = check_every;
+}
