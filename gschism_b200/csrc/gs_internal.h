@@ -1,0 +1,111 @@
+// Internal declarations of gschism_b200 (host C++ and CUDA).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/gschism_b200.h"
+
+#include <vector_types.h>   // double2 (plain struct, usable from host-only translation units)
+
+namespace gs {
+
+struct Connectivity {
+    std::vector<int32_t> nne_start, nne, nnp_start, nnp, ic3, elside, isdel, isidenode;
+    int ns = 0;
+};
+int build_connectivity(int np, int ne, const int32_t* elnode, const int32_t* i34, const int32_t* isbnd,
+                       Connectivity& c);
+void hilbert_order(int n, const double* x, const double* y, std::vector<int32_t>& perm);
+
+constexpr int kMaxTracers = 8;
+constexpr int kMaxLevels = 64;
+constexpr int kMaxBfr = 8;
+constexpr int kMaxDeg = 24;        // max node degree supported by the per-row assembly
+
+// Device error bits (gs_stats.error_flags)
+enum : int {
+    ERR_BARRIER_TIMEOUT = 1,
+    ERR_JCG_NOT_CONVERGED = 2,
+    ERR_DEGREE = 4,
+};
+
+// Batch-wide constants shared by all members (copied into kernel arguments).
+struct Phys {
+    int nvrt, ntr, nz;
+    double h_s, h_c, theta_f;
+    double dt, thetai, h0, dtb_min, dtb_max, velmin, rmaxvel, dfv0, coricoef, rho0, grav, dramp;
+    int ihhat;
+};
+
+// Device state of a batch: members concatenated entity-wise, SFC order inside each member.
+// Per-level fields are level-major: f[k * N + i].
+struct Dev {
+    int NP, NE, NS, NNZ, NB, nmem;
+    // nodes
+    double *x, *y, *depth, *drag, *tau, *eta1, *eta2, *qel, *elbc;
+    int32_t *kb;
+    uint8_t *ndry, *nwas, *ess;
+    int32_t *nbnd;                 // -1 interior, -2 land-only, >= 0 open
+    double *z, *w2, *tr;           // [nvrt][NP], [ntr][nvrt][NP]
+    double2 *u2;                   // [nvrt][NP]
+    int32_t *nne_s, *nne, *nne_loc; // node -> elements (CCW) and the node's local index there
+    int32_t *nnp_s, *nnp, *nbr_slot, *diag_slot;
+    int32_t *sb1, *sb2;            // open-boundary node -> linked boundary sides
+    // open boundary nodes (elevation BC)
+    int32_t *bn_node, *bn_ietype, *bn_nbfr;
+    double *bn_emo, *bn_efa, *bn_amig, *bn_ff, *bn_face;   // [NB][kMaxBfr]
+    // CSR of the elevation matrix (rows = nodes)
+    int32_t *indptr, *indices;
+    double *A;
+    float *A32;
+    // JCG vectors
+    double *b, *xs, *r, *zz, *p0, *p1, *q, *invD, *xh0, *xh1, *xh2;
+    float *r32, *z32, *p032, *p132, *q32, *d32, *invD32;
+    // sides
+    int32_t *sn, *se;              // [2][NS]
+    double *len, *snx, *sny, *scx, *scy, *cori;
+    int32_t *kbs;
+    uint8_t *sdry;
+    int8_t *sbt;                   // 0 interior, 1 land, 2 open
+    double *zc, *Qh;               // [nvrt][NS]
+    double2 *su2, *btu;            // [nvrt][NS]
+    int32_t *btel;                 // [nvrt][NS]
+    double2 *U, *gE1, *gE2;
+    double *hhat, *chi, *chi2;
+    // elements
+    int32_t *en, *es;              // [3][NE]
+    double *area;
+    double2 *gphi;                 // [3][NE]
+    int8_t *ssgn;                  // [3][NE]
+    int32_t *kbe;
+    uint8_t *edry;
+    double *ez, *ew, *Qv;          // [nvrt][NE]
+    double *etr, *prev;            // [ntr][nvrt][NE]
+    double *maxDt;
+    double2 *ghat;
+    // members
+    int32_t *mem_np0, *mem_ne0;    // entity offsets [nmem+1]
+    int32_t *elem_member;          // [NE]
+    double *mem_rem, *mem_dtb;     // transport sub-cycling per member
+    unsigned long long *mem_mindt; // positive doubles ordered as unsigned
+    int32_t *mem_nsub;
+    // JCG work list: tiles of rows inside one member
+    int ntiles;
+    int32_t *tile_r0, *tile_r1, *tile_mem, *mem_t0, *mem_t1;
+    double *tile_part;             // [4][ntiles] partial sums
+    double *mem_scal;              // per member scalars (see jcg.cu)
+    int32_t *mem_iters, *mem_outer;
+    // global control
+    unsigned *bar_count, *bar_gen;
+    int32_t *err;
+    unsigned long long *counters;  // [4]: walk cap hits, btrack stops, ...
+};
+
+}  // namespace gs
+
+#ifdef __CUDACC__
+#define GS_HD __host__ __device__ __forceinline__
+#else
+#define GS_HD inline
+#endif

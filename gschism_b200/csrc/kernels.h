@@ -1,0 +1,51 @@
+// Launch entry points of the gschism_b200 kernels (host side).
+#pragma once
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "gs_internal.h"
+
+namespace gs {
+
+struct VG;
+
+struct JcgArgs {
+    int n, precision;
+    const int32_t *indptr, *indices;
+    const double* A;
+    const float* A32;
+    const double *b, *invD;
+    double *x, *r, *z, *q, *p0, *p1;
+    float *r32, *z32, *q32, *p032, *p132, *d32, *invD32;
+    unsigned *bar_count, *bar_gen;
+    int32_t* err;
+    double rtol;
+    int maxiter, check_every;
+    double inner_rtol;
+    int inner_maxiter;
+};
+struct JcgWork;
+cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std::vector<int>& rows);
+void jcg_work_free(JcgWork* w);
+cudaError_t jcg_launch(const JcgArgs& a, JcgWork* w, cudaStream_t st, int nsm);
+cudaError_t jcg_read_iters(JcgWork* w, std::vector<int>& iters, std::vector<int>& outer, cudaStream_t st);
+int32_t* jcg_iters_device(JcgWork* w);
+
+// k_elev.cu
+void launch_elev_prepare(const Dev& d, const Phys& P, double time, double ramp, cudaStream_t st, int nsm);
+void launch_assemble(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
+void launch_update_elev(const Dev& d, const VG& vg, cudaStream_t st, int nsm);
+// k_btrack.cu
+void launch_btrack(const Dev& d, const Phys& P, const VG& vg, cudaStream_t st, int nsm);
+// k_mom.cu
+void launch_momentum(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
+void launch_vvel(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
+// k_transport.cu
+cudaError_t launch_transport(const Dev& d, const Phys& P, double dt, cudaStream_t st, int nsm);
+// k_levels.cu
+void launch_geometry(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
+void launch_levels(const Dev& d, const Phys& P, const VG& vg, int it, cudaStream_t st, int nsm);
+void launch_nodal_vel(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
+
+}  // namespace gs

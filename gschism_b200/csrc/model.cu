@@ -1,0 +1,750 @@
+// Context of gschism_b200: batch set-up, device state, phases of the step, CUDA-graph step,
+// state exchange in reference numbering, and the stand-alone CSR JCG solver.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dev_common.cuh"
+#include "kernels.h"
+
+using namespace gs;
+
+namespace {
+
+struct MemberHost {
+    // input copy (reference numbering)
+    int np = 0, ne = 0, nope = 0, nland = 0, nbfr = 0;
+    std::vector<double> x, y, depth, drag, tau, tr_init;
+    std::vector<int32_t> elnode, open_start, open_nodes, land_start, land_nodes, iettype;
+    std::vector<double> amig, ff, face, emo, efa;
+    // derived
+    Connectivity con;
+    std::vector<int32_t> isbnd;
+    std::vector<int32_t> pn, pe, ps;      // new -> old
+    std::vector<int32_t> qn, qe, qs;      // old -> new
+    int nnz = 0;
+    int np0 = 0, ne0 = 0, ns0 = 0, nnz0 = 0, nb0 = 0;   // batch offsets
+    std::vector<int32_t> csr_row_perm;    // helper for CSR export
+};
+
+struct HostBatch {
+    // concatenated arrays in batch (new) numbering
+    std::vector<double> x, y, depth, drag, tau, eta;
+    std::vector<int32_t> nbnd, nne_s, nne, nne_loc, nnp_s, nnp, nbr_slot, diag_slot, sb1, sb2;
+    std::vector<uint8_t> ess;
+    std::vector<int32_t> indptr, indices;
+    std::vector<int32_t> sn, se;         // [2][NS]
+    std::vector<double> len, snx, sny, scx, scy, cori;
+    std::vector<int8_t> sbt;
+    std::vector<int32_t> en, es;         // [3][NE]
+    std::vector<double> area, gphi;      // gphi: [3][NE] x,y interleaved
+    std::vector<int8_t> ssgn;
+    std::vector<int32_t> elem_member, mem_np0, mem_ne0;
+    std::vector<int32_t> bn_node, bn_ietype, bn_nbfr;
+    std::vector<double> bn_emo, bn_efa, bn_amig, bn_ff, bn_face;
+    std::vector<double> tr, etr;         // [ntr][nvrt][NP], [ntr][nvrt][NE]
+};
+
+}  // namespace
+
+struct gs_ctx {
+    gs_config cfg{};
+    std::vector<double> ztot, sigma;
+    std::vector<MemberHost> mem;
+    bool finalized = false;
+    int dev = 0, nsm = 148;
+    cudaStream_t st = nullptr;
+    Dev d{};
+    VG vg{};
+    Phys P{};
+    JcgWork* jw = nullptr;
+    std::vector<void*> allocs;
+    int it = 0;
+    cudaGraphExec_t graph = nullptr;
+    int32_t* d_it = nullptr;
+    std::string err;
+    std::vector<int> last_iters, last_outer;
+    gs_status fail(gs_status s, const std::string& m) { err = m; return s; }
+};
+
+namespace {
+
+template <typename T>
+cudaError_t dalloc(gs_ctx* c, T*& p, size_t n) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, (n ? n : 1) * sizeof(T));
+    if (e == cudaSuccess) { cudaMemset(q, 0, (n ? n : 1) * sizeof(T)); c->allocs.push_back(q); p = (T*)q; }
+    return e;
+}
+
+template <typename T>
+cudaError_t dup(gs_ctx* c, T*& p, const std::vector<T>& h) {
+    cudaError_t e = dalloc(c, p, h.size());
+    if (e == cudaSuccess && !h.empty()) e = cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+}
+
+void compute_isbnd(MemberHost& m) {
+    // open nodes carry their segment index (last wins), land-only nodes -2, interior -1
+    m.isbnd.assign(m.np, -1);
+    for (int k = 0; k < m.nope; k++)
+        for (int j = m.open_start[k]; j < m.open_start[k + 1]; j++) m.isbnd[m.open_nodes[j]] = k;
+    for (int k = 0; k < m.nland; k++)
+        for (int j = m.land_start[k]; j < m.land_start[k + 1]; j++)
+            if (m.isbnd[m.land_nodes[j]] == -1) m.isbnd[m.land_nodes[j]] = -2;
+}
+
+int seg_of_pair(const std::vector<int32_t>& start, const std::vector<int32_t>& nodes, int nseg, int a, int b) {
+    for (int k = 0; k < nseg; k++)
+        for (int j = start[k]; j < start[k + 1] - 1; j++) {
+            const int b1 = nodes[j], b2 = nodes[j + 1];
+            if ((b1 == a && b2 == b) || (b1 == b && b2 == a)) return k;
+        }
+    return -1;
+}
+
+}  // namespace
+
+// ============================================================================ C ABI ====
+
+extern "C" {
+
+gs_status gs_ctx_create(const gs_config* cfg, gs_ctx** out) {
+    if (!cfg || !out) return GS_ERR_ARG;
+    if (cfg->nvrt < 2 || cfg->nvrt > kMaxLevels || cfg->ntr < 0 || cfg->ntr > kMaxTracers || cfg->nz < 1 ||
+        cfg->nz > cfg->nvrt)
+        return GS_ERR_ARG;
+    gs_ctx* c = new gs_ctx();
+    c->cfg = *cfg;
+    c->ztot.assign(cfg->ztot, cfg->ztot + cfg->nz);
+    c->sigma.assign(cfg->sigma, cfg->sigma + (cfg->nvrt - cfg->nz + 1));
+    c->cfg.ztot = c->ztot.data();
+    c->cfg.sigma = c->sigma.data();
+    if (c->cfg.check_every < 1) c->cfg.check_every = 1;
+    if (c->cfg.maxiter < 1) c->cfg.maxiter = 1;
+    if (c->cfg.ir_inner_maxiter < 1) c->cfg.ir_inner_maxiter = 200;
+    if (!(c->cfg.ir_inner_rtol > 0.0)) c->cfg.ir_inner_rtol = 1e-4;
+    *out = c;
+    return GS_OK;
+}
+
+gs_status gs_member_add(gs_ctx* c, const gs_member_desc* m, int* id) {
+    if (!c || !m || c->finalized) return GS_ERR_ARG;
+    if (m->np < 3 || m->ne < 1 || m->nbfr < 0 || m->nbfr > kMaxBfr) return c->fail(GS_ERR_ARG, "bad member sizes");
+    MemberHost h;
+    h.np = m->np; h.ne = m->ne; h.nope = m->nope; h.nland = m->nland; h.nbfr = m->nbfr;
+    const int nvrt = c->cfg.nvrt, ntr = c->cfg.ntr;
+    h.x.assign(m->x, m->x + m->np); h.y.assign(m->y, m->y + m->np); h.depth.assign(m->depth, m->depth + m->np);
+    h.drag.assign(m->drag, m->drag + m->np); h.tau.assign(m->tau, m->tau + 2 * (size_t)m->np);
+    h.tr_init.assign(m->tr_init, m->tr_init + (size_t)ntr * nvrt * m->np);
+    h.elnode.assign(m->elnode, m->elnode + 3 * (size_t)m->ne);
+    h.open_start.assign(m->open_start, m->open_start + m->nope + 1);
+    const int non = m->nope ? m->open_start[m->nope] : 0;
+    h.open_nodes.assign(m->open_nodes, m->open_nodes + non);
+    h.land_start.assign(m->land_start, m->land_start + m->nland + 1);
+    h.land_nodes.assign(m->land_nodes, m->land_nodes + (m->nland ? m->land_start[m->nland] : 0));
+    h.iettype.assign(m->iettype, m->iettype + m->nope);
+    h.amig.assign(m->amig, m->amig + m->nbfr); h.ff.assign(m->ff, m->ff + m->nbfr); h.face.assign(m->face, m->face + m->nbfr);
+    h.emo.assign(m->emo, m->emo + (size_t)non * m->nbfr); h.efa.assign(m->efa, m->efa + (size_t)non * m->nbfr);
+    for (int v : h.elnode) if (v < 0 || v >= m->np) return c->fail(GS_ERR_ARG, "element node out of range");
+    *id = (int)c->mem.size();
+    c->mem.push_back(std::move(h));
+    return GS_OK;
+}
+
+const char* gs_last_error(const gs_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+}  // extern "C"
+
+// ----------------------------------------------------------------------- finalize ----
+
+static gs_status build_member(gs_ctx* c, MemberHost& m, HostBatch& B, int mid) {
+    const int nvrt = c->cfg.nvrt, ntr = c->cfg.ntr;
+    compute_isbnd(m);
+    std::vector<int32_t> el4(4 * (size_t)m.ne, -1), i34(m.ne, 3);
+    for (int e = 0; e < m.ne; e++)
+        for (int j = 0; j < 3; j++) el4[4 * e + j] = m.elnode[3 * e + j];
+    if (build_connectivity(m.np, m.ne, el4.data(), i34.data(), m.isbnd.data(), m.con) != 0)
+        return c->fail(GS_ERR_BAD_MESH, "mesh connectivity check failed");
+    const Connectivity& C = m.con;
+    const int np = m.np, ne = m.ne, ns = C.ns;
+    // space-filling-curve order of nodes, elements (centroids) and sides (midpoints)
+    hilbert_order(np, m.x.data(), m.y.data(), m.pn);
+    {
+        std::vector<double> cx(ne), cy(ne);
+        for (int e = 0; e < ne; e++) {
+            cx[e] = (m.x[m.elnode[3 * e]] + m.x[m.elnode[3 * e + 1]] + m.x[m.elnode[3 * e + 2]]) / 3.0;
+            cy[e] = (m.y[m.elnode[3 * e]] + m.y[m.elnode[3 * e + 1]] + m.y[m.elnode[3 * e + 2]]) / 3.0;
+        }
+        hilbert_order(ne, cx.data(), cy.data(), m.pe);
+        std::vector<double> sx(ns), sy(ns);
+        for (int s = 0; s < ns; s++) {
+            sx[s] = 0.5 * (m.x[C.isidenode[2 * s]] + m.x[C.isidenode[2 * s + 1]]);
+            sy[s] = 0.5 * (m.y[C.isidenode[2 * s]] + m.y[C.isidenode[2 * s + 1]]);
+        }
+        hilbert_order(ns, sx.data(), sy.data(), m.ps);
+    }
+    m.qn.assign(np, 0); m.qe.assign(ne, 0); m.qs.assign(ns, 0);
+    for (int i = 0; i < np; i++) m.qn[m.pn[i]] = i;
+    for (int i = 0; i < ne; i++) m.qe[m.pe[i]] = i;
+    for (int i = 0; i < ns; i++) m.qs[m.ps[i]] = i;
+    const int NP0 = (int)B.x.size(), NE0 = (int)B.area.size(), NS0 = (int)B.len.size();
+    m.np0 = NP0; m.ne0 = NE0; m.ns0 = NS0;
+    m.nnz0 = (int)B.indices.size();
+    // nodes
+    for (int i = 0; i < np; i++) {
+        const int o = m.pn[i];
+        B.x.push_back(m.x[o]); B.y.push_back(m.y[o]); B.depth.push_back(m.depth[o]); B.drag.push_back(m.drag[o]);
+        B.tau.push_back(m.tau[2 * o]); B.tau.push_back(m.tau[2 * o + 1]);
+        B.nbnd.push_back(m.isbnd[o]);
+    }
+    // node -> elements with the node's local index, node -> nodes, CSR rows sorted by column
+    for (int i = 0; i < np; i++) {
+        const int o = m.pn[i];
+        for (int q = C.nne_start[o]; q < C.nne_start[o + 1]; q++) {
+            const int eo = C.nne[q];
+            int loc = -1;
+            for (int j = 0; j < 3; j++) if (m.elnode[3 * eo + j] == o) loc = j;
+            B.nne.push_back(NE0 + m.qe[eo]);
+            B.nne_loc.push_back(loc);
+        }
+        B.nne_s.push_back((int)B.nne.size());
+        const int rs = (int)B.indices.size();
+        std::vector<std::pair<int, int>> cols;   // (new column, position in the ball or -1 for diag)
+        const int s0 = C.nnp_start[o], s1 = C.nnp_start[o + 1];
+        if (s1 - s0 > kMaxDeg) return c->fail(GS_ERR_BAD_MESH, "node degree above the supported maximum");
+        cols.push_back({i, -1});
+        for (int a = s0; a < s1; a++) cols.push_back({m.qn[C.nnp[a]], a - s0});
+        std::sort(cols.begin(), cols.end());
+        std::vector<int32_t> slot(s1 - s0, 0);
+        int dslot = 0;
+        for (size_t r = 0; r < cols.size(); r++) {
+            B.indices.push_back(NP0 + cols[r].first);
+            if (cols[r].second < 0) dslot = rs + (int)r;
+            else slot[cols[r].second] = rs + (int)r;
+        }
+        B.diag_slot.push_back(dslot);
+        for (int a = s0; a < s1; a++) { B.nnp.push_back(NP0 + m.qn[C.nnp[a]]); B.nbr_slot.push_back(slot[a - s0]); }
+        B.nnp_s.push_back((int)B.nnp.size());
+        B.indptr.push_back((int)B.indices.size());
+        B.sb1.push_back(-1); B.sb2.push_back(-1);
+        B.ess.push_back(0);
+    }
+    m.nnz = (int)B.indices.size() - m.nnz0;
+    // open boundary nodes: the last matching (segment, position) provides the constituents
+    std::vector<int> bn_pos(np, -1);
+    for (int k = 0; k < m.nope; k++)
+        for (int j = m.open_start[k]; j < m.open_start[k + 1]; j++) {
+            const int o = m.open_nodes[j];
+            B.ess[NP0 + m.qn[o]] = (m.iettype[k] != 0);
+            bn_pos[o] = j;
+        }
+    m.nb0 = (int)B.bn_node.size();
+    for (int i = 0; i < np; i++) {
+        const int o = m.pn[i];
+        if (m.isbnd[o] < 0) continue;
+        const int j = bn_pos[o];
+        B.bn_node.push_back(NP0 + i);
+        B.bn_ietype.push_back(m.iettype[m.isbnd[o]]);
+        B.bn_nbfr.push_back(m.nbfr);
+        for (int f = 0; f < kMaxBfr; f++) {
+            const bool ok = f < m.nbfr && j >= 0;
+            B.bn_emo.push_back(ok ? m.emo[(size_t)j * m.nbfr + f] : 0.0);
+            B.bn_efa.push_back(ok ? m.efa[(size_t)j * m.nbfr + f] : 0.0);
+            B.bn_amig.push_back(f < m.nbfr ? m.amig[f] : 0.0);
+            B.bn_ff.push_back(f < m.nbfr ? m.ff[f] : 0.0);
+            B.bn_face.push_back(f < m.nbfr ? m.face[f] : 0.0);
+        }
+    }
+    // sides (geometry as populateSides, meshdata.cu:2146-2347; boundary type and open-node links
+    // in reference side order)
+    std::vector<int8_t> sbt_old(ns, 0);
+    std::vector<int32_t> sb1(np, -1), sb2(np, -1);
+    for (int s = 0; s < ns; s++) {
+        const int a = C.isidenode[2 * s], b = C.isidenode[2 * s + 1];
+        if (m.isbnd[a] != -1 && m.isbnd[b] != -1) {
+            if (seg_of_pair(m.land_start, m.land_nodes, m.nland, a, b) >= 0) sbt_old[s] = 1;
+            else if (seg_of_pair(m.open_start, m.open_nodes, m.nope, a, b) >= 0) sbt_old[s] = 2;
+            if (sbt_old[s]) {
+                const int nn[2] = {a, b};
+                for (int qq = 0; qq < 2; qq++) {
+                    const int i = nn[qq];
+                    if (m.isbnd[i] < 0) continue;
+                    if (sb1[i] < 0) sb1[i] = s; else if (sb2[i] < 0) sb2[i] = s;
+                }
+            }
+        }
+    }
+    for (int i = 0; i < np; i++) {
+        const int o = m.pn[i];
+        B.sb1[NP0 + i] = sb1[o] >= 0 ? NS0 + m.qs[sb1[o]] : -1;
+        B.sb2[NP0 + i] = sb2[o] >= 0 ? NS0 + m.qs[sb2[o]] : -1;
+    }
+    for (int s = 0; s < ns; s++) {
+        const int so = m.ps[s];
+        const int a = C.isidenode[2 * so], b = C.isidenode[2 * so + 1];
+        const int e0 = C.isdel[2 * so], e1 = C.isdel[2 * so + 1];
+        B.sn.push_back(NP0 + m.qn[a]);
+        B.se.push_back(e0 >= 0 ? NE0 + m.qe[e0] : -1);
+        B.scx.push_back(0.5 * (m.x[a] + m.x[b]));
+        B.scy.push_back(0.5 * (m.y[a] + m.y[b]));
+        const double nx = -(m.y[a] - m.y[b]), ny = (m.x[a] - m.x[b]);
+        const double ln = std::sqrt(nx * nx + ny * ny);
+        B.snx.push_back(nx / ln); B.sny.push_back(ny / ln);
+        const double dx = m.x[b] - m.x[a], dy = m.y[b] - m.y[a], dz = 0.0 - 0.0;
+        B.len.push_back(std::sqrt(dx * dx + dy * dy + dz * dz));
+        B.cori.push_back(c->cfg.coricoef);
+        B.sbt.push_back(sbt_old[so]);
+        (void)e1;
+    }
+    // second rows of the [2][NS] side arrays are appended after all members (see finalize)
+    // elements (populateElements, meshdata.cu:2350-2480)
+    for (int e = 0; e < ne; e++) {
+        const int eo = m.pe[e];
+        const int* nd = &m.elnode[3 * eo];
+        const double x0 = m.x[nd[0]], y0 = m.y[nd[0]], x1 = m.x[nd[1]], y1 = m.y[nd[1]], x2 = m.x[nd[2]], y2 = m.y[nd[2]];
+        const double area = 0.5 * ((x0 - x2) * (y1 - y2) - (x1 - x2) * (y0 - y2));
+        B.area.push_back(area);
+        B.elem_member.push_back(mid);
+    }
+    (void)nvrt; (void)ntr;
+    return GS_OK;
+}
+
+extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
+    if (!c || c->finalized) return GS_ERR_ARG;
+    if (c->mem.empty()) return c->fail(GS_ERR_ARG, "no members");
+    cudaError_t ce = cudaSetDevice(c->cfg.device);
+    if (ce != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(ce));
+    c->dev = c->cfg.device;
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->dev);
+    if (!coop) return c->fail(GS_ERR_CUDA, "device lacks cooperative launch");
+    const int nvrt = c->cfg.nvrt, ntr = c->cfg.ntr;
+    HostBatch B;
+    B.nne_s.push_back(0); B.nnp_s.push_back(0); B.indptr.push_back(0);
+    for (size_t k = 0; k < c->mem.size(); k++) {
+        B.mem_np0.push_back((int)B.x.size());
+        B.mem_ne0.push_back((int)B.area.size());
+        gs_status s = build_member(c, c->mem[k], B, (int)k);
+        if (s != GS_OK) return s;
+    }
+    const int NP = (int)B.x.size(), NE = (int)B.area.size(), NS = (int)B.len.size();
+    B.mem_np0.push_back(NP); B.mem_ne0.push_back(NE);
+    // second halves of [2][NS] and the [3][NE] arrays, geometry of elements, initial tracers
+    std::vector<int32_t> sn2(NS), se2(NS);
+    std::vector<int32_t> en(3 * (size_t)NE), es(3 * (size_t)NE);
+    std::vector<double> gphi(6 * (size_t)NE);
+    std::vector<int8_t> ssg(3 * (size_t)NE);
+    B.tr.assign((size_t)ntr * nvrt * NP, 0.0);
+    B.etr.assign((size_t)ntr * nvrt * NE, 0.0);
+    for (auto& m : c->mem) {
+        const Connectivity& C = m.con;
+        for (int s = 0; s < C.ns; s++) {
+            const int so = m.ps[s];
+            sn2[m.ns0 + s] = m.np0 + m.qn[C.isidenode[2 * so + 1]];
+            const int e1 = C.isdel[2 * so + 1];
+            se2[m.ns0 + s] = e1 >= 0 ? m.ne0 + m.qe[e1] : -1;
+        }
+        for (int e = 0; e < m.ne; e++) {
+            const int eo = m.pe[e], E = m.ne0 + e;
+            const int* nd = &m.elnode[3 * eo];
+            const double area = B.area[E];
+            for (int j = 0; j < 3; j++) {
+                en[(size_t)j * NE + E] = m.np0 + m.qn[nd[j]];
+                const int so = C.elside[4 * eo + j];
+                es[(size_t)j * NE + E] = m.ns0 + m.qs[so];
+                ssg[(size_t)j * NE + E] = (C.isdel[2 * so] == eo) ? 1 : -1;
+                const int p2 = nd[(j + 1) % 3], p3 = nd[(j + 2) % 3];
+                gphi[2 * ((size_t)j * NE + E)] = (m.y[p2] - m.y[p3]) / (2 * area);
+                gphi[2 * ((size_t)j * NE + E) + 1] = (m.x[p3] - m.x[p2]) / (2 * area);
+            }
+            // initial element tracers: node levels k and k-1 averaged, level 0 = level 1
+            const double inv = 1.0 / (2.0 * 3);
+            for (int t = 0; t < ntr; t++) {
+                for (int k = 1; k < nvrt; k++) {
+                    double sum = 0.0;
+                    for (int j = 0; j < 3; j++)
+                        sum += m.tr_init[((size_t)t * nvrt + k) * m.np + nd[j]] +
+                               m.tr_init[((size_t)t * nvrt + k - 1) * m.np + nd[j]];
+                    B.etr[((size_t)t * nvrt + k) * NE + E] = inv * sum;
+                }
+                B.etr[((size_t)t * nvrt + 0) * NE + E] = B.etr[((size_t)t * nvrt + 1) * NE + E];
+            }
+        }
+        for (int t = 0; t < ntr; t++)
+            for (int k = 0; k < nvrt; k++)
+                for (int i = 0; i < m.np; i++)
+                    B.tr[((size_t)t * nvrt + k) * NP + m.np0 + i] = m.tr_init[((size_t)t * nvrt + k) * m.np + m.pn[i]];
+    }
+    B.sn.insert(B.sn.end(), sn2.begin(), sn2.end());
+    B.se.insert(B.se.end(), se2.begin(), se2.end());
+
+    // ------------------------------------------------------------------ device state
+    Dev& d = c->d;
+    d.NP = NP; d.NE = NE; d.NS = NS; d.NNZ = (int)B.indices.size(); d.NB = (int)B.bn_node.size();
+    d.nmem = (int)c->mem.size();
+    cudaError_t e = cudaSuccess;
+#define UP(field, vec) if (e == cudaSuccess) e = dup(c, d.field, vec)
+#define AL(field, n) if (e == cudaSuccess) e = dalloc(c, d.field, n)
+    UP(x, B.x); UP(y, B.y); UP(depth, B.depth); UP(drag, B.drag); UP(tau, B.tau);
+    AL(eta1, NP); AL(eta2, NP); AL(qel, NP); AL(elbc, NP); AL(kb, NP); AL(ndry, NP); AL(nwas, NP);
+    UP(ess, B.ess); UP(nbnd, B.nbnd);
+    AL(z, (size_t)nvrt * NP); AL(w2, (size_t)nvrt * NP); AL(u2, (size_t)nvrt * NP);
+    UP(tr, B.tr);
+    UP(nne_s, B.nne_s); UP(nne, B.nne); UP(nne_loc, B.nne_loc); UP(nnp_s, B.nnp_s); UP(nnp, B.nnp);
+    UP(nbr_slot, B.nbr_slot); UP(diag_slot, B.diag_slot); UP(sb1, B.sb1); UP(sb2, B.sb2);
+    UP(bn_node, B.bn_node); UP(bn_ietype, B.bn_ietype); UP(bn_nbfr, B.bn_nbfr);
+    UP(bn_emo, B.bn_emo); UP(bn_efa, B.bn_efa); UP(bn_amig, B.bn_amig); UP(bn_ff, B.bn_ff); UP(bn_face, B.bn_face);
+    UP(indptr, B.indptr); UP(indices, B.indices); AL(A, d.NNZ); AL(A32, d.NNZ);
+    AL(b, NP); AL(xs, NP); AL(r, NP); AL(zz, NP); AL(p0, NP); AL(p1, NP); AL(q, NP); AL(invD, NP);
+    AL(xh0, NP); AL(xh1, NP); AL(xh2, NP);
+    AL(r32, NP); AL(z32, NP); AL(p032, NP); AL(p132, NP); AL(q32, NP); AL(d32, NP); AL(invD32, NP);
+    UP(sn, B.sn); UP(se, B.se); UP(len, B.len); UP(snx, B.snx); UP(sny, B.sny); UP(scx, B.scx); UP(scy, B.scy);
+    UP(cori, B.cori); AL(kbs, NS); AL(sdry, NS); UP(sbt, B.sbt);
+    AL(zc, (size_t)nvrt * NS); AL(Qh, (size_t)nvrt * NS); AL(su2, (size_t)nvrt * NS); AL(btu, (size_t)nvrt * NS);
+    AL(btel, (size_t)nvrt * NS); AL(U, NS); AL(gE1, NS); AL(gE2, NS); AL(hhat, NS); AL(chi, NS); AL(chi2, NS);
+    UP(en, en); UP(es, es); UP(area, B.area);
+    if (e == cudaSuccess) { e = dalloc(c, d.gphi, 3 * (size_t)NE); if (e == cudaSuccess) e = cudaMemcpy(d.gphi, gphi.data(), gphi.size() * 8, cudaMemcpyHostToDevice); }
+    UP(ssgn, ssg); AL(kbe, NE); AL(edry, NE);
+    AL(ez, (size_t)nvrt * NE); AL(ew, (size_t)nvrt * NE); AL(Qv, (size_t)nvrt * NE);
+    UP(etr, B.etr); AL(prev, (size_t)ntr * nvrt * NE); AL(maxDt, NE); AL(ghat, NE);
+    UP(mem_np0, B.mem_np0); UP(mem_ne0, B.mem_ne0); UP(elem_member, B.elem_member);
+    AL(mem_rem, 2 * (size_t)d.nmem); AL(mem_dtb, d.nmem); AL(mem_mindt, 2 * (size_t)d.nmem + 1); AL(mem_nsub, d.nmem);
+    AL(bar_count, 1); AL(bar_gen, 1); AL(err, 1); AL(counters, 4);
+#undef UP
+#undef AL
+    if (e != cudaSuccess) return c->fail(e == cudaErrorMemoryAllocation ? GS_ERR_OOM : GS_ERR_CUDA, cudaGetErrorString(e));
+    {
+        std::vector<int> row0, rows;
+        for (auto& m : c->mem) { row0.push_back(m.np0); rows.push_back(m.np); }
+        e = jcg_work_alloc(c->jw, row0, rows);
+        if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    // constants
+    Phys& P = c->P;
+    const gs_config& g = c->cfg;
+    P.nvrt = nvrt; P.ntr = ntr; P.nz = g.nz; P.h_s = g.h_s; P.h_c = g.h_c; P.theta_f = g.theta_f;
+    P.dt = g.dt; P.thetai = g.thetai; P.h0 = g.h0; P.dtb_min = g.dtb_min; P.dtb_max = g.dtb_max;
+    P.velmin = g.velmin_btrack; P.rmaxvel = g.rmaxvel; P.dfv0 = g.dfv0; P.coricoef = g.coricoef;
+    P.rho0 = g.rho0; P.grav = g.grav; P.dramp = g.dramp; P.ihhat = g.ihhat;
+    VG& vg = c->vg;
+    std::memset(&vg, 0, sizeof(vg));
+    vg.nvrt = nvrt; vg.nz = g.nz; vg.h_s = g.h_s; vg.h_c = g.h_c; vg.h0 = g.h0;
+    for (int k = 0; k < g.nz; k++) vg.ztot[k] = c->ztot[k];
+    for (int k = 0; k < nvrt - g.nz + 1; k++) {
+        const double s = c->sigma[k], tb = g.theta_b, tf = g.theta_f;
+        vg.sigma[k] = s;
+        vg.cs[k] = (1.0 - tb) * std::sinh(tf * s) / std::sinh(tf) +
+                   tb * (std::tanh(tf * (s + 0.5)) - std::tanh(tf * 0.5)) / 2.0 / std::tanh(tf * 0.5);
+    }
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return c->fail(GS_ERR_CUDA, "stream");
+    // cold start levels (schism_init.py:81-91)
+    launch_levels(c->d, c->P, c->vg, 0, c->st, c->nsm);
+    e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    c->finalized = true;
+    return GS_OK;
+}
+
+// ------------------------------------------------------------------------- phases ----
+
+static double ramp_of(const gs_ctx* c, double time) {
+    return (c->cfg.dramp > 0.0) ? std::tanh(2.0 * time / 86400.0 / c->cfg.dramp) : 1.0;
+}
+
+static gs_status run_phase(gs_ctx* c, int phase, int arg) {
+    const int nsm = c->nsm;
+    cudaStream_t st = c->st;
+    const double time = c->it * c->cfg.dt;
+    switch (phase) {
+    case GS_PHASE_BEGIN: c->it = arg; break;
+    case GS_PHASE_BTRACK: launch_btrack(c->d, c->P, c->vg, st, nsm); break;
+    case GS_PHASE_PREPARE: launch_elev_prepare(c->d, c->P, time, ramp_of(c, time), st, nsm); break;
+    case GS_PHASE_ASSEMBLE:
+        launch_assemble(c->d, c->P, st, nsm);
+        break;
+    case GS_PHASE_SOLVE: {
+        JcgArgs a{};
+        Dev& d = c->d;
+        a.n = d.NP; a.precision = c->cfg.precision;
+        a.indptr = d.indptr; a.indices = d.indices; a.A = d.A; a.A32 = d.A32; a.b = d.b; a.invD = d.invD;
+        a.x = d.xs; a.r = d.r; a.z = d.zz; a.q = d.q; a.p0 = d.p0; a.p1 = d.p1;
+        a.r32 = d.r32; a.z32 = d.z32; a.q32 = d.q32; a.p032 = d.p032; a.p132 = d.p132; a.d32 = d.d32; a.invD32 = d.invD32;
+        a.bar_count = d.bar_count; a.bar_gen = d.bar_gen; a.err = d.err;
+        a.rtol = c->cfg.rtol; a.maxiter = c->cfg.maxiter; a.check_every = c->cfg.check_every;
+        a.inner_rtol = c->cfg.ir_inner_rtol; a.inner_maxiter = c->cfg.ir_inner_maxiter;
+        cudaError_t e = jcg_launch(a, c->jw, st, nsm);
+        if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, std::string("jcg launch: ") + cudaGetErrorString(e));
+        break;
+    }
+    case GS_PHASE_UPDATE_ELEV: launch_update_elev(c->d, c->vg, st, nsm); break;
+    case GS_PHASE_MOMENTUM: launch_momentum(c->d, c->P, st, nsm); break;
+    case GS_PHASE_VVEL: launch_vvel(c->d, c->P, st, nsm); break;
+    case GS_PHASE_TRANSPORT: {
+        cudaError_t e = launch_transport(c->d, c->P, c->cfg.dt, st, nsm);
+        if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, std::string("transport launch: ") + cudaGetErrorString(e));
+        break;
+    }
+    case GS_PHASE_LEVELS: launch_levels(c->d, c->P, c->vg, arg, st, nsm); break;
+    case GS_PHASE_NODAL_VEL: launch_nodal_vel(c->d, c->P, st, nsm); break;
+    default: return c->fail(GS_ERR_ARG, "unknown phase");
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    return GS_OK;
+}
+
+static gs_status check_err(gs_ctx* c) {
+    int32_t flags = 0;
+    cudaError_t e = cudaMemcpyAsync(&flags, c->d.err, 4, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    if (flags & ERR_BARRIER_TIMEOUT) return c->fail(GS_ERR_TIMEOUT, "a bounded device barrier timed out");
+    if (flags & ERR_DEGREE) return c->fail(GS_ERR_BAD_MESH, "node degree above the supported maximum");
+    return GS_OK;
+}
+
+extern "C" {
+
+gs_status gs_phase(gs_ctx* c, int phase, int arg) {
+    if (!c || !c->finalized) return GS_ERR_ARG;
+    return run_phase(c, phase, arg);
+}
+
+gs_status gs_step(gs_ctx* c, int nsteps) {
+    if (!c || !c->finalized || nsteps < 0) return GS_ERR_ARG;
+    for (int n = 0; n < nsteps; n++) {
+        const int it = c->it + 1;
+        const int seq[] = {GS_PHASE_BTRACK, GS_PHASE_PREPARE, GS_PHASE_ASSEMBLE, GS_PHASE_SOLVE, GS_PHASE_UPDATE_ELEV,
+                           GS_PHASE_MOMENTUM, GS_PHASE_VVEL, GS_PHASE_TRANSPORT, GS_PHASE_LEVELS, GS_PHASE_NODAL_VEL};
+        gs_status s = run_phase(c, GS_PHASE_BEGIN, it);
+        for (int ph : seq) {
+            if (s != GS_OK) return s;
+            s = run_phase(c, ph, it);
+        }
+        if (s != GS_OK) return s;
+    }
+    return GS_OK;
+}
+
+gs_status gs_sync(gs_ctx* c) {
+    if (!c || !c->finalized) return GS_ERR_ARG;
+    return check_err(c);
+}
+
+gs_status gs_member_sizes(gs_ctx* c, int member, int* np, int* ne, int* ns, int* nnz) {
+    if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size()) return GS_ERR_ARG;
+    const MemberHost& m = c->mem[member];
+    *np = m.np; *ne = m.ne; *ns = m.con.ns; *nnz = m.nnz;
+    return GS_OK;
+}
+
+gs_status gs_get_stats(gs_ctx* c, int member, gs_stats* out) {
+    if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size() || !out) return GS_ERR_ARG;
+    gs_status s = check_err(c);
+    std::vector<int> iters, outer;
+    cudaError_t e = jcg_read_iters(c->jw, iters, outer, c->st);
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    unsigned long long cnt[4] = {0, 0, 0, 0};
+    int32_t nsub = 0, flags = 0;
+    cudaMemcpy(cnt, c->d.counters, sizeof(cnt), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&nsub, c->d.mem_nsub + member, 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(&flags, c->d.err, 4, cudaMemcpyDeviceToHost);
+    std::memset(out, 0, sizeof(*out));
+    out->jcg_iters = iters[member];
+    out->jcg_outer = outer[member];
+    out->transport_substeps = nsub;
+    out->walk_cap_hits = (int64_t)cnt[0];
+    out->btrack_stops = (int64_t)cnt[1];
+    out->error_flags = flags;
+    return s == GS_OK ? GS_OK : s;
+}
+
+gs_status gs_ctx_destroy(gs_ctx* c) {
+    if (!c) return GS_ERR_ARG;
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->st) { cudaStreamSynchronize(c->st); cudaStreamDestroy(c->st); }
+    jcg_work_free(c->jw);
+    for (void* p : c->allocs) cudaFree(p);
+    delete c;
+    return GS_OK;
+}
+
+}  // extern "C"
+
+// --------------------------------------------------------------------- state exchange ----
+
+namespace {
+
+struct FieldInfo {
+    char ent;       // 'N', 'S', 'E', 'C' (CSR), 'R' (CSR rows + 1)
+    int lev;        // per-level
+    int comp;       // 1, 2 (vector), -1 tracers
+    int isint;      // 0 double, 1 int32, 2 uint8 (exchanged as int32)
+    void* ptr;
+};
+
+bool field_info(gs_ctx* c, int f, FieldInfo& fi) {
+    Dev& d = c->d;
+    fi = FieldInfo{'N', 0, 1, 0, nullptr};
+    switch (f) {
+    case GS_F_ETA1: fi.ptr = d.eta1; return true;
+    case GS_F_ETA2: fi.ptr = d.eta2; return true;
+    case GS_F_QEL: fi.ptr = d.qel; return true;
+    case GS_F_ELBC: fi.ptr = d.elbc; return true;
+    case GS_F_JCG_X: fi.ptr = d.xh0; return true;
+    case GS_F_JCG_X1: fi.ptr = d.xh1; return true;
+    case GS_F_JCG_X2: fi.ptr = d.xh2; return true;
+    case GS_F_NODE_Z: fi.lev = 1; fi.ptr = d.z; return true;
+    case GS_F_NODE_U2: fi.lev = 1; fi.comp = 2; fi.ptr = d.u2; return true;
+    case GS_F_NODE_W2: fi.lev = 1; fi.ptr = d.w2; return true;
+    case GS_F_NODE_TR: fi.lev = 1; fi.comp = -1; fi.ptr = d.tr; return true;
+    case GS_F_NODE_KB: fi.isint = 1; fi.ptr = d.kb; return true;
+    case GS_F_NODE_DRY: fi.isint = 2; fi.ptr = d.ndry; return true;
+    case GS_F_SIDE_U2: fi.ent = 'S'; fi.lev = 1; fi.comp = 2; fi.ptr = d.su2; return true;
+    case GS_F_SIDE_BTU: fi.ent = 'S'; fi.lev = 1; fi.comp = 2; fi.ptr = d.btu; return true;
+    case GS_F_SIDE_ZC: fi.ent = 'S'; fi.lev = 1; fi.ptr = d.zc; return true;
+    case GS_F_SIDE_QH: fi.ent = 'S'; fi.lev = 1; fi.ptr = d.Qh; return true;
+    case GS_F_SIDE_BTELEM: fi.ent = 'S'; fi.lev = 1; fi.isint = 1; fi.ptr = d.btel; return true;
+    case GS_F_SIDE_KB: fi.ent = 'S'; fi.isint = 1; fi.ptr = d.kbs; return true;
+    case GS_F_SIDE_DRY: fi.ent = 'S'; fi.isint = 2; fi.ptr = d.sdry; return true;
+    case GS_F_SIDE_U: fi.ent = 'S'; fi.comp = 2; fi.ptr = d.U; return true;
+    case GS_F_SIDE_HHAT: fi.ent = 'S'; fi.ptr = d.hhat; return true;
+    case GS_F_SIDE_CHI: fi.ent = 'S'; fi.ptr = d.chi; return true;
+    case GS_F_SIDE_GRADETA1: fi.ent = 'S'; fi.comp = 2; fi.ptr = d.gE1; return true;
+    case GS_F_SIDE_GRADETA2: fi.ent = 'S'; fi.comp = 2; fi.ptr = d.gE2; return true;
+    case GS_F_ELEM_Z: fi.ent = 'E'; fi.lev = 1; fi.ptr = d.ez; return true;
+    case GS_F_ELEM_W: fi.ent = 'E'; fi.lev = 1; fi.ptr = d.ew; return true;
+    case GS_F_ELEM_QV: fi.ent = 'E'; fi.lev = 1; fi.ptr = d.Qv; return true;
+    case GS_F_ELEM_TR: fi.ent = 'E'; fi.lev = 1; fi.comp = -1; fi.ptr = d.etr; return true;
+    case GS_F_ELEM_KB: fi.ent = 'E'; fi.isint = 1; fi.ptr = d.kbe; return true;
+    case GS_F_ELEM_DRY: fi.ent = 'E'; fi.isint = 2; fi.ptr = d.edry; return true;
+    case GS_F_ELEM_GHAT: fi.ent = 'E'; fi.comp = 2; fi.ptr = d.ghat; return true;
+    case GS_F_CSR_DATA: fi.ent = 'C'; fi.ptr = d.A; return true;
+    case GS_F_CSR_INDPTR: fi.ent = 'R'; fi.isint = 1; return true;
+    case GS_F_CSR_INDICES: fi.ent = 'C'; fi.isint = 1; return true;
+    default: return false;
+    }
+}
+
+// reference-numbered CSR of one member: rows in reference node order, columns sorted by
+// reference index, values gathered from the device matrix
+void member_csr(gs_ctx* c, MemberHost& m, std::vector<int32_t>& indptr, std::vector<int32_t>& indices,
+                std::vector<int32_t>& src) {
+    const Connectivity& C = m.con;
+    indptr.assign(m.np + 1, 0);
+    indices.clear(); src.clear();
+    std::vector<int32_t> hind(m.nnz), hptr(m.np + 1);
+    cudaMemcpy(hind.data(), c->d.indices + m.nnz0, 4 * (size_t)m.nnz, cudaMemcpyDeviceToHost);
+    cudaMemcpy(hptr.data(), c->d.indptr + m.np0, 4 * (size_t)(m.np + 1), cudaMemcpyDeviceToHost);
+    for (int o = 0; o < m.np; o++) {
+        const int i = m.qn[o];
+        std::vector<std::pair<int, int>> row;
+        for (int a = hptr[i]; a < hptr[i + 1]; a++) row.push_back({m.pn[hind[a - m.nnz0 + 0] - m.np0], a});
+        std::sort(row.begin(), row.end());
+        for (auto& pr : row) { indices.push_back(pr.first); src.push_back(pr.second); }
+        indptr[o + 1] = (int)indices.size();
+    }
+    (void)C;
+}
+
+}  // namespace
+
+extern "C" gs_status gs_state_get(gs_ctx* c, int member, int field, void* host, size_t bytes) {
+    if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size() || !host) return GS_ERR_ARG;
+    FieldInfo fi;
+    if (!field_info(c, field, fi)) return c->fail(GS_ERR_STATE, "unknown field");
+    MemberHost& m = c->mem[member];
+    const int nvrt = c->cfg.nvrt, ntr = c->cfg.ntr;
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->fail(GS_ERR_CUDA, "sync");
+    if (fi.ent == 'C' || fi.ent == 'R') {
+        std::vector<int32_t> ip, ix, src;
+        member_csr(c, m, ip, ix, src);
+        if (fi.ent == 'R') {
+            if (bytes != 4 * ip.size()) return c->fail(GS_ERR_STATE, "size");
+            std::memcpy(host, ip.data(), bytes);
+        } else if (fi.isint) {
+            if (bytes != 4 * ix.size()) return c->fail(GS_ERR_STATE, "size");
+            std::memcpy(host, ix.data(), bytes);
+        } else {
+            if (bytes != 8 * src.size()) return c->fail(GS_ERR_STATE, "size");
+            std::vector<double> all(m.nnz);
+            cudaMemcpy(all.data(), c->d.A + m.nnz0, 8 * (size_t)m.nnz, cudaMemcpyDeviceToHost);
+            double* out = (double*)host;
+            for (size_t a = 0; a < src.size(); a++) out[a] = all[src[a] - m.nnz0];
+        }
+        return GS_OK;
+    }
+    const int N = fi.ent == 'N' ? c->d.NP : fi.ent == 'S' ? c->d.NS : c->d.NE;
+    const int n = fi.ent == 'N' ? m.np : fi.ent == 'S' ? m.con.ns : m.ne;
+    const int off = fi.ent == 'N' ? m.np0 : fi.ent == 'S' ? m.ns0 : m.ne0;
+    const std::vector<int32_t>& perm = fi.ent == 'N' ? m.pn : fi.ent == 'S' ? m.ps : m.pe;   // new -> old
+    const int nl = fi.lev ? nvrt : 1;
+    const int nc = fi.comp == 2 ? 2 : 1;
+    const int nt = fi.comp == -1 ? ntr : 1;
+    const size_t esz = fi.isint ? 4 : 8;
+    const size_t need = (size_t)nt * nl * n * nc * esz;
+    if (bytes != need) return c->fail(GS_ERR_STATE, "size mismatch for field");
+    const size_t dsz = fi.isint == 2 ? 1 : esz;
+    std::vector<char> buf((size_t)n * nc * dsz);
+    for (int t = 0; t < nt; t++)
+        for (int k = 0; k < nl; k++) {
+            const size_t dev_off = (((size_t)t * nl + k) * N + off) * nc * dsz;
+            cudaMemcpy(buf.data(), (char*)fi.ptr + dev_off, buf.size(), cudaMemcpyDeviceToHost);
+            for (int i = 0; i < n; i++) {
+                const int o = perm[i];
+                const size_t dst = ((((size_t)t * nl + k) * n + o) * nc) * esz;
+                if (fi.isint == 2) ((int32_t*)((char*)host + dst))[0] = (int32_t)(uint8_t)buf[i];
+                else std::memcpy((char*)host + dst, buf.data() + (size_t)i * nc * dsz, nc * dsz);
+            }
+        }
+    return GS_OK;
+}
+
+extern "C" gs_status gs_state_put(gs_ctx* c, int member, int field, const void* host, size_t bytes) {
+    if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size() || !host) return GS_ERR_ARG;
+    FieldInfo fi;
+    if (!field_info(c, field, fi)) return c->fail(GS_ERR_STATE, "unknown field");
+    if (fi.ent == 'C' || fi.ent == 'R') return c->fail(GS_ERR_STATE, "CSR fields are read-only");
+    MemberHost& m = c->mem[member];
+    const int nvrt = c->cfg.nvrt, ntr = c->cfg.ntr;
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->fail(GS_ERR_CUDA, "sync");
+    const int N = fi.ent == 'N' ? c->d.NP : fi.ent == 'S' ? c->d.NS : c->d.NE;
+    const int n = fi.ent == 'N' ? m.np : fi.ent == 'S' ? m.con.ns : m.ne;
+    const int off = fi.ent == 'N' ? m.np0 : fi.ent == 'S' ? m.ns0 : m.ne0;
+    const std::vector<int32_t>& perm = fi.ent == 'N' ? m.pn : fi.ent == 'S' ? m.ps : m.pe;
+    const int nl = fi.lev ? nvrt : 1;
+    const int nc = fi.comp == 2 ? 2 : 1;
+    const int nt = fi.comp == -1 ? ntr : 1;
+    const size_t esz = fi.isint ? 4 : 8;
+    if (bytes != (size_t)nt * nl * n * nc * esz) return c->fail(GS_ERR_STATE, "size mismatch for field");
+    const size_t dsz = fi.isint == 2 ? 1 : esz;
+    std::vector<char> buf((size_t)n * nc * dsz);
+    for (int t = 0; t < nt; t++)
+        for (int k = 0; k < nl; k++) {
+            for (int i = 0; i < n; i++) {
+                const int o = perm[i];
+                const size_t src = ((((size_t)t * nl + k) * n + o) * nc) * esz;
+                if (fi.isint == 2) buf[i] = (char)(uint8_t)((const int32_t*)((const char*)host + src))[0];
+                else std::memcpy(buf.data() + (size_t)i * nc * dsz, (const char*)host + src, nc * dsz);
+            }
+            const size_t dev_off = (((size_t)t * nl + k) * N + off) * nc * dsz;
+            cudaMemcpy((char*)fi.ptr + dev_off, buf.data(), buf.size(), cudaMemcpyHostToDevice);
+        }
+    return GS_OK;
+}
+
+extern "C" gs_status gs_set_tau(gs_ctx* c, int member, const double* tau_host) {
+    if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size() || !tau_host) return GS_ERR_ARG;
+    MemberHost& m = c->mem[member];
+    std::vector<double> buf(2 * (size_t)m.np);
+    for (int i = 0; i < m.np; i++) { buf[2 * i] = tau_host[2 * m.pn[i]]; buf[2 * i + 1] = tau_host[2 * m.pn[i] + 1]; }
+    cudaError_t e = cudaMemcpyAsync(c->d.tau + 2 * (size_t)m.np0, buf.data(), buf.size() * 8, cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    return e == cudaSuccess ? GS_OK : c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+}

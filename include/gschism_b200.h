@@ -1,0 +1,169 @@
+/* gschism_b200: B200-native SCHISM semi-implicit hydrodynamic step, C ABI.
+ *
+ * One context (gs_ctx) holds a batch of ensemble members (independent meshes of any size that
+ * share the vertical grid and the physics constants) resident in the HBM of one GPU.  Every
+ * phase of the step runs as one launch over all members; the whole step is a fixed launch
+ * sequence on the context's stream, captured once in a CUDA graph.
+ *
+ * Conventions: every entry point returns a gs_status (0 = GS_OK) and never aborts the process;
+ * gs_last_error() describes the last failure.  Host pointers are caller-owned and only read
+ * during the call.  Contexts are independent (thread-safe across contexts, not within one).
+ * Field exchange (gs_state_get/put) uses the reference numbering of the member's own input and
+ * level-major layout: per-level fields [nvrt][n], vectors [nvrt][n][2], tracers [ntr][nvrt][n].
+ *
+ * Reference interfaces replaced (paths within schism-dev/gschism):
+ *   src/grid/read_and_process_grid.cpp:829-855   readHGrid connectivity        -> gs_grid_build
+ *   src/solver/pcg_solver.py:538-1148            PCGSolverMultiGPU             -> gs_jcg_*
+ *   src/solver/pcg_loop.cpp:182-291,467-479      NativePCG.add_partition/solve -> gs_jcg_solve_csr
+ *   src/python/schism_step.py:95-334             schism_step                   -> gs_step
+ *   src/python/cuda_functions.py:140-257         cufunc.<kernel>(...)          -> gs_phase
+ *   src/kernels/meshdata.cu:7560-8000            get{Node,Side,Element}Var*    -> gs_state_get/put
+ */
+#ifndef GSCHISM_B200_H
+#define GSCHISM_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int gs_status;
+enum {
+    GS_OK = 0,
+    GS_ERR_ARG = 1,            /* bad argument or call order */
+    GS_ERR_CUDA = 2,           /* CUDA runtime error (message in gs_last_error) */
+    GS_ERR_OOM = 3,            /* device allocation failed */
+    GS_ERR_NOT_CONVERGED = 4,  /* JCG reached maxiter without meeting the tolerance */
+    GS_ERR_TIMEOUT = 5,        /* a bounded device wait gave up (error flag set by a kernel) */
+    GS_ERR_BAD_MESH = 6,       /* connectivity check failed (hanging node, broken ball, ...) */
+    GS_ERR_STATE = 7           /* field or member unknown, or buffer size mismatch */
+};
+
+enum { GS_FP64 = 0, GS_FP32_IR = 1 };   /* JCG precision: plain FP64, or FP32 inner + FP64 refinement */
+
+/* ------------------------------------------------------------------ grid ---- */
+
+/* Mesh connectivity exactly as readHGrid builds it (read_and_process_grid.cpp:27-574):
+ * node->elements in counter-clockwise order, element-side-element table ic3, side numbering,
+ * isdel/isidenode, node->nodes in counter-clockwise order.
+ * elnode[ne*4] (-1 padded), i34[ne], isbnd[np] (open segment index, -2 land, -1 interior).
+ * Output capacities: nne[4*ne], nnp[4*ne+np], ic3/elside[4*ne], isdel/isidenode[2*4*ne]. */
+gs_status gs_grid_build(int np, int ne, const int32_t* elnode, const int32_t* i34, const int32_t* isbnd,
+                        int32_t* nne_start, int32_t* nne, int32_t* nnp_start, int32_t* nnp,
+                        int32_t* ic3, int32_t* elside, int32_t* isdel, int32_t* isidenode,
+                        int32_t* ns_out);
+
+/* ------------------------------------------------------------------ model ---- */
+
+typedef struct {
+    int nvrt, ntr;                         /* levels and tracers (shared by all members) */
+    int nz; double h_s, h_c, theta_b, theta_f;
+    const double* ztot;                    /* [nz], ztot[nz-1] = -h_s (vgrid.in, ivcor = 2) */
+    const double* sigma;                   /* [nvrt-nz+1] */
+    double dt, thetai, h0, dtb_min, dtb_max, velmin_btrack, rmaxvel, dfv0, coricoef, rho0, grav, dramp;
+    int ihhat;
+    double rtol; int maxiter, check_every; /* JCG: pcg_solver.py:1075 solve(rtol, maxiter, checkEvery) */
+    int precision;                         /* GS_FP64 or GS_FP32_IR */
+    double ir_inner_rtol;                  /* FP32 inner solve: stop at this relative residual */
+    int ir_inner_maxiter;
+    int device;                            /* CUDA device ordinal */
+} gs_config;
+
+typedef struct {
+    int np, ne, nope, nland, nbfr;
+    const double* x; const double* y; const double* depth;
+    const double* drag;                    /* [np] bottom drag coefficient (nchi = 0) */
+    const double* tau;                     /* [np][2] kinematic surface stress, m^2/s^2 */
+    const double* tr_init;                 /* [ntr][nvrt][np] initial nodal tracers */
+    const int32_t* elnode;                 /* [ne][3] counter-clockwise triangles */
+    const int32_t* open_start;             /* [nope+1] */
+    const int32_t* open_nodes;
+    const int32_t* land_start;             /* [nland+1] */
+    const int32_t* land_nodes;
+    const int32_t* iettype;                /* [nope]: 0 none, 3 tidal harmonics */
+    const double* amig; const double* ff; const double* face;   /* [nbfr] */
+    const double* emo; const double* efa;  /* [open_start[nope]][nbfr] in open_nodes order */
+} gs_member_desc;
+
+typedef struct gs_ctx gs_ctx;
+
+gs_status gs_ctx_create(const gs_config* cfg, gs_ctx** out);
+gs_status gs_member_add(gs_ctx* ctx, const gs_member_desc* desc, int* member_id);
+/* Allocate device state for every added member, upload, build geometry and cold-start levels. */
+gs_status gs_ctx_finalize(gs_ctx* ctx);
+gs_status gs_ctx_destroy(gs_ctx* ctx);
+const char* gs_last_error(const gs_ctx* ctx);
+gs_status gs_sync(gs_ctx* ctx);
+
+/* Advance every member by nsteps steps (schism_step.py:95-334), as CUDA-graph launches. */
+gs_status gs_step(gs_ctx* ctx, int nsteps);
+
+/* Individual phases of one step, in call order (the cufunc kernels of schism_step.py). */
+enum {
+    GS_PHASE_BEGIN = 0,        /* time ramps and forcing for step `it` (arg) */
+    GS_PHASE_BTRACK = 1,       /* backtrackAllNodes, meshdata.cu:3547 */
+    GS_PHASE_PREPARE = 2,      /* elevation BCs, U, hhat/chi, ghat1 (meshdata.cu:4276-4725, 6183) */
+    GS_PHASE_ASSEMBLE = 3,     /* setupCoefficientMatrixAndRHS + rollUp + setEssentialBC */
+    GS_PHASE_SOLVE = 4,        /* solveWaveEquation (JCG) */
+    GS_PHASE_UPDATE_ELEV = 5,  /* updateElevation */
+    GS_PHASE_MOMENTUM = 6,     /* computeHorGradientAtSide, solveMomentumEquations, applyMomentumBC */
+    GS_PHASE_VVEL = 7,         /* computeVerticalVelocity */
+    GS_PHASE_TRANSPORT = 8,    /* computeTransport(dt) */
+    GS_PHASE_LEVELS = 9,       /* ul0* wet/dry and levels (arg = it) */
+    GS_PHASE_NODAL_VEL = 10    /* nodal velocities */
+};
+gs_status gs_phase(gs_ctx* ctx, int phase, int arg);
+
+/* State exchange in reference numbering (see the header comment for layouts). */
+enum {
+    GS_F_ETA1 = 0, GS_F_ETA2 = 1, GS_F_NODE_Z = 2, GS_F_NODE_U2 = 3, GS_F_NODE_W2 = 4,
+    GS_F_NODE_TR = 5, GS_F_NODE_KB = 6, GS_F_NODE_DRY = 7, GS_F_QEL = 8,
+    GS_F_SIDE_U2 = 10, GS_F_SIDE_BTU = 11, GS_F_SIDE_ZC = 12, GS_F_SIDE_KB = 13, GS_F_SIDE_DRY = 14,
+    GS_F_SIDE_U = 15, GS_F_SIDE_HHAT = 16, GS_F_SIDE_CHI = 17, GS_F_SIDE_QH = 18,
+    GS_F_SIDE_BTELEM = 19, GS_F_SIDE_GRADETA1 = 20, GS_F_SIDE_GRADETA2 = 21,
+    GS_F_ELEM_Z = 30, GS_F_ELEM_W = 31, GS_F_ELEM_QV = 32, GS_F_ELEM_TR = 33, GS_F_ELEM_KB = 34,
+    GS_F_ELEM_DRY = 35, GS_F_ELEM_GHAT = 36,
+    GS_F_CSR_DATA = 40, GS_F_CSR_INDPTR = 41, GS_F_CSR_INDICES = 42, GS_F_JCG_X = 43, GS_F_ELBC = 44,
+    GS_F_JCG_X1 = 45, GS_F_JCG_X2 = 46   /* JCG solution history x0 (last), x1, x2 */
+};
+/* bytes must equal the field's size (int32 for *_KB, *_DRY, SIDE_BTELEM, CSR_INDPTR/INDICES). */
+gs_status gs_state_get(gs_ctx* ctx, int member, int field, void* host, size_t bytes);
+gs_status gs_state_put(gs_ctx* ctx, int member, int field, const void* host, size_t bytes);
+/* Per-step host forcing: replace a member's surface stress [np][2] (host buffer, copied). */
+gs_status gs_set_tau(gs_ctx* ctx, int member, const double* tau_host);
+
+typedef struct {
+    int64_t jcg_iters;         /* iterations of the last solve (inner FP32 iterations for IR) */
+    int64_t jcg_outer;         /* FP64 refinement sweeps of the last solve (IR) */
+    double jcg_relres;         /* |b - Ax| / |b| of the last solve (FP64) */
+    int64_t transport_substeps;
+    int64_t walk_cap_hits;     /* celestial walks that reached 40 iterations */
+    int64_t btrack_stops;      /* backtracks stopped at the 38th sub-step */
+    int32_t error_flags;       /* device error bits (bounded waits, non-convergence) */
+} gs_stats;
+gs_status gs_get_stats(gs_ctx* ctx, int member, gs_stats* out);
+/* sizes of a member: np, ne, ns, nnz (CSR of the elevation matrix) */
+gs_status gs_member_sizes(gs_ctx* ctx, int member, int* np, int* ne, int* ns, int* nnz);
+
+/* ------------------------------------------------------------------ JCG on a caller CSR ---- */
+
+/* Stand-alone Jacobi-PCG on one CSR matrix, with the semantics of PCGSolverMultiGPU.solve
+ * (pcg_solver.py:1075-1124): b, x live in solver-owned device buffers; the solve computes
+ * invD = 1/diag(A), atol = rtol*|b|, the parabolic guess x = 3x0 - 3x1 + x2 from the previous
+ * three solutions, iterates, and rolls the history.  Device pointers returned by gs_jcg_buffers
+ * are owned by the solver and stay valid until gs_jcg_destroy. */
+typedef struct gs_jcg gs_jcg;
+gs_status gs_jcg_create(int n, int nnz, int precision, int device, gs_jcg** out);
+gs_status gs_jcg_buffers(gs_jcg* s, int32_t** indptr, int32_t** indices, double** data,
+                         double** b, double** x);
+gs_status gs_jcg_solve_csr(gs_jcg* s, double rtol, int maxiter, int check_every, int* iters);
+/* |b - A x| / |b| of the current solution (pcg_solver.py:1127-1143) */
+gs_status gs_jcg_check(gs_jcg* s, double* relres);
+gs_status gs_jcg_destroy(gs_jcg* s);
+const char* gs_jcg_last_error(const gs_jcg* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -16,6 +16,8 @@ static void* fptr(const og_model* m, int f, fdesc* d) {
     case OGF_QEL: d->n = m->np; return m->qel;
     case OGF_ELBC: d->n = m->np; return m->elbc;
     case OGF_JCG_X: d->n = m->np; return m->x0;
+    case OGF_JCG_X1: d->n = m->np; return m->x1;
+    case OGF_JCG_X2: d->n = m->np; return m->x2;
     case OGF_NODE_Z: d->n = m->np; d->lev = 1; return m->z;
     case OGF_NODE_U2: d->n = m->np; d->lev = 1; d->comp = 2; return m->u2;
     case OGF_NODE_W2: d->n = m->np; d->lev = 1; return m->w2;

@@ -46,7 +46,7 @@ enum {
     OGF_ELEM_Z = 30, OGF_ELEM_W = 31, OGF_ELEM_QV = 32, OGF_ELEM_TR = 33, OGF_ELEM_KB = 34,
     OGF_ELEM_DRY = 35, OGF_ELEM_GHAT = 36,
     OGF_CSR_DATA = 40, OGF_CSR_INDPTR = 41, OGF_CSR_INDICES = 42, OGF_JCG_X = 43,
-    OGF_ELBC = 44
+    OGF_ELBC = 44, OGF_JCG_X1 = 45, OGF_JCG_X2 = 46
 };
 
 typedef struct og_model og_model;

@@ -17,7 +17,7 @@ F = dict(ETA1=0, ETA2=1, NODE_Z=2, NODE_U2=3, NODE_W2=4, NODE_TR=5, NODE_KB=6, N
          SIDE_U2=10, SIDE_BTU=11, SIDE_ZC=12, SIDE_KB=13, SIDE_DRY=14, SIDE_U=15, SIDE_HHAT=16,
          SIDE_CHI=17, SIDE_QH=18, SIDE_BTELEM=19, SIDE_GRADETA1=20, SIDE_GRADETA2=21,
          ELEM_Z=30, ELEM_W=31, ELEM_QV=32, ELEM_TR=33, ELEM_KB=34, ELEM_DRY=35, ELEM_GHAT=36,
-         CSR_DATA=40, CSR_INDPTR=41, CSR_INDICES=42, JCG_X=43, ELBC=44)
+         CSR_DATA=40, CSR_INDPTR=41, CSR_INDICES=42, JCG_X=43, ELBC=44, JCG_X1=45, JCG_X2=46)
 INT_FIELDS = {"NODE_KB", "NODE_DRY", "SIDE_KB", "SIDE_DRY", "SIDE_BTELEM", "ELEM_KB", "ELEM_DRY",
               "CSR_INDPTR", "CSR_INDICES"}
 
@@ -135,7 +135,7 @@ class OracleModel:
     # -------------------------------------------------------------- state exchange
     def shape(self, name: str):
         n = {"N": self.np, "S": self.ns, "E": self.ne}
-        per = {"ETA1": ("N",), "ETA2": ("N",), "QEL": ("N",), "ELBC": ("N",), "JCG_X": ("N",),
+        per = {"ETA1": ("N",), "ETA2": ("N",), "QEL": ("N",), "ELBC": ("N",), "JCG_X": ("N",), "JCG_X1": ("N",), "JCG_X2": ("N",),
                "NODE_KB": ("N",), "NODE_DRY": ("N",), "SIDE_KB": ("S",), "SIDE_DRY": ("S",),
                "SIDE_HHAT": ("S",), "SIDE_CHI": ("S",), "ELEM_KB": ("E",), "ELEM_DRY": ("E",)}
         if name in per:
