@@ -23,7 +23,7 @@ PHASE = dict(BEGIN=0, BTRACK=1, PREPARE=2, ASSEMBLE=3, SOLVE=4, UPDATE_ELEV=5, M
              TRANSPORT=8, LEVELS=9, NODAL_VEL=10)
 
 EXPORTS = ["gs_grid_build", "gs_ctx_create", "gs_member_add", "gs_ctx_finalize", "gs_ctx_destroy",
-           "gs_last_error", "gs_sync", "gs_step", "gs_phase", "gs_state_get", "gs_state_put", "gs_set_tau",
+           "gs_last_error", "gs_sync", "gs_set_stream", "gs_step", "gs_phase", "gs_state_get", "gs_state_put", "gs_set_tau",
            "gs_get_stats", "gs_member_sizes", "gs_jcg_create", "gs_jcg_buffers", "gs_jcg_solve_csr",
            "gs_jcg_check", "gs_jcg_destroy", "gs_jcg_last_error"]
 
@@ -80,6 +80,7 @@ def load(build_if_missing: bool = False):
     L.gs_last_error.argtypes = [c_void_p]
     L.gs_last_error.restype = ctypes.c_char_p
     L.gs_sync.argtypes = [c_void_p]
+    L.gs_set_stream.argtypes = [c_void_p, c_void_p]
     L.gs_step.argtypes = [c_void_p, I]
     L.gs_phase.argtypes = [c_void_p, I, I]
     L.gs_state_get.argtypes = [c_void_p, I, I, c_void_p, c_size_t]

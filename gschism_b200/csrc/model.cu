@@ -57,6 +57,7 @@ struct gs_ctx {
     bool finalized = false;
     int dev = 0, nsm = 148;
     cudaStream_t st = nullptr;
+    cudaStream_t own_st = nullptr;
     Dev d{};
     VG vg{};
     Phys P{};
@@ -442,7 +443,8 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
         vg.cs[k] = (1.0 - tb) * std::sinh(tf * s) / std::sinh(tf) +
                    tb * (std::tanh(tf * (s + 0.5)) - std::tanh(tf * 0.5)) / 2.0 / std::tanh(tf * 0.5);
     }
-    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return c->fail(GS_ERR_CUDA, "stream");
+    if (cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking) != cudaSuccess) return c->fail(GS_ERR_CUDA, "stream");
+    c->st = c->own_st;
     // cold start levels (schism_init.py:81-91)
     launch_levels(c->d, c->P, c->vg, 0, c->st, c->nsm);
     e = cudaStreamSynchronize(c->st);
@@ -537,6 +539,13 @@ gs_status gs_sync(gs_ctx* c) {
     return check_err(c);
 }
 
+gs_status gs_set_stream(gs_ctx* c, void* stream) {
+    if (!c || !c->finalized) return GS_ERR_ARG;
+    cudaStreamSynchronize(c->st);
+    c->st = stream ? (cudaStream_t)stream : c->own_st;
+    return GS_OK;
+}
+
 gs_status gs_member_sizes(gs_ctx* c, int member, int* np, int* ne, int* ns, int* nnz) {
     if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size()) return GS_ERR_ARG;
     const MemberHost& m = c->mem[member];
@@ -568,7 +577,8 @@ gs_status gs_get_stats(gs_ctx* c, int member, gs_stats* out) {
 gs_status gs_ctx_destroy(gs_ctx* c) {
     if (!c) return GS_ERR_ARG;
     if (c->graph) cudaGraphExecDestroy(c->graph);
-    if (c->st) { cudaStreamSynchronize(c->st); cudaStreamDestroy(c->st); }
+    if (c->st) cudaStreamSynchronize(c->st);
+    if (c->own_st) cudaStreamDestroy(c->own_st);
     jcg_work_free(c->jw);
     for (void* p : c->allocs) cudaFree(p);
     delete c;
@@ -701,6 +711,10 @@ extern "C" gs_status gs_state_get(gs_ctx* c, int member, int field, void* host, 
                 const size_t dst = ((((size_t)t * nl + k) * n + o) * nc) * esz;
                 if (fi.isint == 2) ((int32_t*)((char*)host + dst))[0] = (int32_t)(uint8_t)buf[i];
                 else std::memcpy((char*)host + dst, buf.data() + (size_t)i * nc * dsz, nc * dsz);
+                if (field == GS_F_SIDE_BTELEM) {       // element ids back to reference numbering
+                    int32_t* v = (int32_t*)((char*)host + dst);
+                    if (*v >= 0) *v = m.pe[*v - m.ne0];
+                }
             }
         }
     return GS_OK;

@@ -130,6 +130,10 @@ class Model:
     def phase(self, name: str, arg: int = 0) -> None:
         L.check(self.lib.gs_phase(self.h, L.PHASE[name], int(arg)), self.h, f"gs_phase {name}")
 
+    def set_stream(self, stream_ptr: int | None) -> None:
+        """Issue the member work on a caller cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""
+        L.check(self.lib.gs_set_stream(self.h, ctypes.c_void_p(stream_ptr or None)), self.h, "gs_set_stream")
+
     def sync(self) -> None:
         L.check(self.lib.gs_sync(self.h), self.h, "gs_sync")
 

@@ -95,6 +95,10 @@ gs_status gs_ctx_finalize(gs_ctx* ctx);
 gs_status gs_ctx_destroy(gs_ctx* ctx);
 const char* gs_last_error(const gs_ctx* ctx);
 gs_status gs_sync(gs_ctx* ctx);
+/* Run the context's work on a caller-owned cudaStream_t (passed as void*; NULL restores the
+ * context's own stream).  Lets a caller order the step with its own work and time it with
+ * events recorded on that stream. */
+gs_status gs_set_stream(gs_ctx* ctx, void* stream);
 
 /* Advance every member by nsteps steps (schism_step.py:95-334), as CUDA-graph launches. */
 gs_status gs_step(gs_ctx* ctx, int nsteps);

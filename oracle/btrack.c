@@ -67,6 +67,7 @@ static int celestial_walk(og_model* m, int* cur, v2 x0, v2 xt, int* lastCross) {
         if (nxt < 0 || m->edry[nxt]) { *cur = prev; return 0; }
         *cur = nxt;
     }
+#pragma omp atomic
     m->cnt[2]++;
     return 1;
 }
@@ -192,7 +193,12 @@ static void side_btrack(og_model* m, int s, int jlev, double dt, double dtbk, do
         if (vmag2 <= m->velmin * m->velmin) { *elem_out = cur; return; }
         x0[0] = xt[0]; x0[1] = xt[1]; x0[2] = xt[2];
         iter++;
-        if (iter == 38) { m->cnt[3]++; *elem_out = cur; return; }     /* mdc:1610-1611 */
+        if (iter == 38) {                                            /* mdc:1610-1611 */
+#pragma omp atomic
+            m->cnt[3]++;
+            *elem_out = cur;
+            return;
+        }
         t3 = t2; t2 = t1; t1 = time_rm;
     }
     interp_vel(m, cur, xt[0], xt[1], xt[2], u_int);
@@ -207,6 +213,7 @@ void og_btrack(og_model* m) {
     const int ndelt_min = (int)fmax(1.0, dt / m->dtb_max);
     const double vm2 = m->velmin * m->velmin;
     m->cnt[2] = 0; m->cnt[3] = 0;
+#pragma omp parallel for schedule(dynamic, 64)
     for (int s = 0; s < m->ns; s++) {
         for (int k = 0; k < nvrt; k++) {
             m->btu[(size_t)s * nvrt + k] = m->su2[(size_t)s * nvrt + k];

@@ -500,6 +500,7 @@ void og_assemble(og_model* m, double time) {
     /* setupCoefficientMatrixAndRHS, mdc:3182-3474 (triangles, imm = 0, ifltype = 0) */
     (void)time;
     const double dt = m->dt, th = m->thetai;
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < m->np; i++) {
         for (int a = m->indptr[i]; a < m->indptr[i + 1]; a++) m->data[a] = 0.0;
         double qel = 0.0;
@@ -690,14 +691,10 @@ void og_momentum(og_model* m, double time) {
         m->gE1[s] = side_grad(m, s, m->eta1, 1);
         m->gE2[s] = side_grad(m, s, m->eta2, 2);
     }
-    double* alow = (double*)malloc(sizeof(double) * nvrt);
-    double* cupp = (double*)malloc(sizeof(double) * nvrt);
-    double* bdia = (double*)malloc(sizeof(double) * nvrt);
-    double* rrhs = (double*)malloc(sizeof(double) * 2 * nvrt);
-    double* soln = (double*)malloc(sizeof(double) * 2 * nvrt);
-    double* gam = (double*)malloc(sizeof(double) * nvrt);
     /* solveMomentumEquations, mdc:5076-5354 */
+#pragma omp parallel for schedule(static)
     for (int s = 0; s < ns; s++) {
+        double alow[nvrt], cupp[nvrt], bdia[nvrt], rrhs[2 * nvrt], soln[2 * nvrt], gam[nvrt];
         v2* u2 = &m->su2[(size_t)s * nvrt];
         const v2* btu = &m->btu[(size_t)s * nvrt];
         if (m->sdry[s]) {
@@ -775,7 +772,6 @@ void og_momentum(og_model* m, double time) {
         else if (!side_is2d(m, s)) u2[kb] = V2(0.0, 0.0);
         for (int k = 0; k < kb; k++) u2[k] = V2(0.0, 0.0);
     }
-    free(alow); free(cupp); free(bdia); free(rrhs); free(soln); free(gam);
     /* applyMomentumBC, mdc:5357-5454: free slip on land sides (islip = 0) */
     for (int s = 0; s < ns; s++) {
         if (m->sbt[s] != 1) continue;
@@ -816,6 +812,7 @@ static void elem_normal(const og_model* m, int e, int k, double* nx, double* ny,
 void og_vertical_velocity(og_model* m) {
     /* computeVerticalVelocity, mdc:5978-6103 (imm = 0, ics = 1) */
     const int nvrt = m->nvrt;
+#pragma omp parallel for schedule(static)
     for (int e = 0; e < m->ne; e++) {
         double* w = &m->ew[(size_t)e * nvrt];
         double* Qv = &m->Qv[(size_t)e * nvrt];
@@ -974,6 +971,7 @@ void og_nodal_velocities(og_model* m) {
     /* zeroNodalVelocities .. computeNodalHorizontalVelocities2, mdc:5765-5929, as a
      * node-centred gather in counter-clockwise element order (indvel <= 0, triangles) */
     const int nvrt = m->nvrt;
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < m->np; i++) {
         double* w2 = &m->w2[(size_t)i * nvrt];
         v2* u2 = &m->u2[(size_t)i * nvrt];

@@ -49,6 +49,7 @@ int og_transport(og_model* m, double dt) {
     int nsub = 0;
     while (remaining > 0.0) {
         /* horizontalAdvectionPrepare */
+#pragma omp parallel for schedule(static)
         for (int e = 0; e < ne; e++) {
             if (m->edry[e]) continue;
             const int kb = m->kbe[e];
@@ -77,6 +78,7 @@ int og_transport(og_model* m, double dt) {
         for (int e = 0; e < ne; e++) mdt = fmin(mdt, m->edry[e] ? HUGE_D : m->maxDt[e]);
         const double dtb = fmin(remaining, mdt);
         /* horizontalAdvectionUpdate(dtb) */
+#pragma omp parallel for schedule(static)
         for (int e = 0; e < ne; e++) {
             if (m->edry[e]) continue;
             const int kb = m->kbe[e];
@@ -116,13 +118,9 @@ int og_transport(og_model* m, double dt) {
     }
     m->cnt[1] = nsub;
     /* verticalAdvectionUpdate(dt) */
-    double* alow = (double*)malloc(sizeof(double) * nvrt);
-    double* bdia = (double*)malloc(sizeof(double) * nvrt);
-    double* cupp = (double*)malloc(sizeof(double) * nvrt);
-    double* rrhs = (double*)malloc(sizeof(double) * nvrt);
-    double* soln = (double*)malloc(sizeof(double) * nvrt);
-    double* gam = (double*)malloc(sizeof(double) * nvrt);
+#pragma omp parallel for schedule(static)
     for (int e = 0; e < ne; e++) {
+        double alow[nvrt], bdia[nvrt], cupp[nvrt], rrhs[nvrt], soln[nvrt], gam[nvrt];
         if (m->edry[e]) continue;
         const int kb = m->kbe[e];
         double* tr = &m->etr[(size_t)e * nvrt * ntr];
@@ -152,9 +150,9 @@ int og_transport(og_model* m, double dt) {
         for (int k = 0; k <= kb; k++)
             for (int t = 0; t < ntr; t++) tr[k * ntr + t] = tr[(kb + 1) * ntr + t];
     }
-    free(alow); free(bdia); free(cupp); free(rrhs); free(soln); free(gam);
     /* nodalTracerUpdate */
     const int ivrt = nvrt - 1;
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < m->np; i++) {
         if (m->ndry[i]) continue;
         for (int k = 0; k < nvrt; k++) {

@@ -1,0 +1,153 @@
+"""CUDA path vs the CPU oracle (gpu).
+
+Per phase: both sides start from the bit-identical state of the oracle after a few steps of the
+10 km channel case (the state is copied into the GPU member in reference numbering), then run
+the same phases of one step.  Integer outputs (backtracked element ids, bottom levels, wet/dry
+flags) must match exactly; FP64 fields within the stated relative tolerances (the CUDA kernels
+contract multiply-adds, the oracle does not; the JCG reductions use a different order).
+"""
+import numpy as np
+import pytest
+
+from gschism_b200 import cases
+from tests._parity import copy_state, level_mask, relerr
+
+pytestmark = pytest.mark.gpu
+
+TOL_PHASE = 1e-12     # single phase from identical inputs (FMA contraction only)
+TOL_SOLVE = 1e-10     # after the JCG solve (reduction order; rtol = 1e-12)
+
+
+@pytest.fixture(scope="module")
+def channel_pair(native, oracle_lib):
+    from gschism_b200.model import Model
+    from oracle.step_api import OracleModel
+    c = cases.channel()
+    o = OracleModel(c)
+    o.run(4)
+    g = Model([c])
+    copy_state(o, g)
+    return c, o, g
+
+
+def test_phases_match_oracle_from_identical_state(channel_pair):
+    c, o, g = channel_pair
+    it = 5
+    dt = c.params.dt
+    nv = c.nvrt
+    # backtracking first: inputs bit-identical, element ids must match exactly
+    o.begin_step(it); g.phase("BEGIN", it)
+    o.btrack(); g.phase("BTRACK", it)
+    assert np.array_equal(g.get(0, "SIDE_BTELEM"), o.get("SIDE_BTELEM"))
+    assert relerr(g.get(0, "SIDE_BTU"), o.get("SIDE_BTU")) <= TOL_PHASE
+    n_walks = int((o.get("SIDE_BTELEM") >= 0).sum())
+    assert n_walks > 1000
+    o.prepare_elevation(it * dt); g.phase("PREPARE", it)
+    assert relerr(g.get(0, "ELBC"), o.get("ELBC")) <= 1e-14
+    assert relerr(g.get(0, "SIDE_U"), o.get("SIDE_U")) <= TOL_PHASE
+    assert relerr(g.get(0, "SIDE_HHAT"), o.get("SIDE_HHAT")) <= TOL_PHASE
+    assert relerr(g.get(0, "ELEM_GHAT"), o.get("ELEM_GHAT")) <= TOL_PHASE
+    o.assemble(it * dt); o.essential_bc(); g.phase("ASSEMBLE", it)
+    assert np.array_equal(g.get(0, "CSR_INDPTR"), o.get("CSR_INDPTR"))
+    assert np.array_equal(g.get(0, "CSR_INDICES"), o.get("CSR_INDICES"))
+    assert relerr(g.get(0, "CSR_DATA"), o.get("CSR_DATA")) <= TOL_PHASE
+    assert relerr(g.get(0, "QEL"), o.get("QEL")) <= TOL_PHASE
+    its_o, _ = o.jcg_solve(c.params.rtol, c.params.maxiter, c.params.check_every)
+    g.phase("SOLVE", it)
+    assert g.stats(0)["jcg_iters"] == its_o
+    o.update_elevation(); g.phase("UPDATE_ELEV", it)
+    assert relerr(g.get(0, "ETA2"), o.get("ETA2")) <= TOL_SOLVE
+    assert np.array_equal(g.get(0, "NODE_KB"), o.get("NODE_KB"))
+    # continue from the oracle's solution so the later phases again see identical inputs
+    copy_state(o, g)
+    o.momentum(it * dt); g.phase("MOMENTUM", it)
+    assert relerr(g.get(0, "SIDE_U2"), o.get("SIDE_U2")) <= TOL_PHASE
+    assert relerr(g.get(0, "SIDE_GRADETA2"), o.get("SIDE_GRADETA2")) <= TOL_PHASE
+    o.vertical_velocity(); g.phase("VVEL", it)
+    kbe = o.get("ELEM_KB")
+    assert relerr(g.get(0, "ELEM_W"), o.get("ELEM_W")) <= 1e-11
+    assert relerr(g.get(0, "ELEM_QV"), o.get("ELEM_QV"), level_mask(kbe, nv)) <= 1e-11
+    o.transport(dt); g.phase("TRANSPORT", it)
+    assert g.stats(0)["transport_substeps"] == o.counters()[1]
+    assert relerr(g.get(0, "SIDE_QH"), o.get("SIDE_QH")) <= TOL_PHASE
+    assert relerr(g.get(0, "ELEM_TR"), o.get("ELEM_TR")) <= TOL_PHASE
+    assert relerr(g.get(0, "NODE_TR"), o.get("NODE_TR")) <= TOL_PHASE
+    o.levels(it); g.phase("LEVELS", it)
+    for f in ("NODE_KB", "NODE_DRY", "ELEM_KB", "ELEM_DRY", "SIDE_KB", "SIDE_DRY"):
+        assert np.array_equal(g.get(0, f), o.get(f)), f
+    kb = o.get("NODE_KB")
+    assert relerr(g.get(0, "NODE_Z"), o.get("NODE_Z"), level_mask(kb, nv)) <= TOL_PHASE
+    assert relerr(g.get(0, "ELEM_Z"), o.get("ELEM_Z"), level_mask(o.get("ELEM_KB"), nv)) <= TOL_PHASE
+    assert relerr(g.get(0, "SIDE_ZC"), o.get("SIDE_ZC"), level_mask(o.get("SIDE_KB"), nv)) <= TOL_PHASE
+    o.nodal_velocities(); g.phase("NODAL_VEL", it)
+    assert relerr(g.get(0, "NODE_U2"), o.get("NODE_U2")) <= TOL_PHASE
+    assert relerr(g.get(0, "NODE_W2"), o.get("NODE_W2")) <= 1e-11
+
+
+def test_btrack_ids_bit_exact_on_basin(native, oracle_lib):
+    """SZ levels, irregular bathymetry: every backtracked element id equals the oracle's."""
+    from gschism_b200.model import Model
+    from oracle.step_api import OracleModel
+    c = cases.basin(seed=9, n=48, nvrt=12, nz=4, ntr=1, length=48e3, amp=1.5)
+    o = OracleModel(c)
+    o.run(3)
+    g = Model([c])
+    copy_state(o, g)
+    o.begin_step(4); g.phase("BEGIN", 4)
+    o.btrack(); g.phase("BTRACK", 4)
+    ids = o.get("SIDE_BTELEM")
+    assert (ids >= 0).sum() > 10000
+    assert np.array_equal(g.get(0, "SIDE_BTELEM"), ids)
+    assert relerr(g.get(0, "SIDE_BTU"), o.get("SIDE_BTU")) <= TOL_PHASE
+
+
+def test_multistep_channel_fp64(native, oracle_lib):
+    """Whole steps through gs_step against og_step.  Elevation and tracers stay within 1e-10
+    relative after 30 steps; velocities within 1e-8 (each solve differs from the oracle's at the
+    1e-12 level through the reduction order, and the momentum solve amplifies that slowly)."""
+    from gschism_b200.model import Model
+    from oracle.step_api import OracleModel
+    c = cases.channel(seed=3)
+    o = OracleModel(c)
+    g = Model([c])
+    n = 30
+    its_o = o.run(n)
+    g.step(n)
+    assert relerr(g.get(0, "ETA2"), o.get("ETA2")) <= 1e-10
+    assert relerr(g.get(0, "SIDE_U2"), o.get("SIDE_U2")) <= 1e-8
+    assert relerr(g.get(0, "ELEM_TR"), o.get("ELEM_TR")) <= 1e-10
+    assert relerr(g.get(0, "NODE_TR"), o.get("NODE_TR")) <= 1e-10
+    assert abs(g.stats(0)["jcg_iters"] - its_o[-1]) <= c.params.check_every
+
+
+def test_batch_members_independent_of_the_mix(native):
+    """Each member's state after several steps is bit-identical alone and inside a batch."""
+    from gschism_b200.model import Model
+    a = cases.channel(seed=11, nx=40, ny=21, nvrt=10)
+    b = cases.channel(seed=12, nx=63, ny=32, nvrt=10)
+    d = cases.channel(seed=13, nx=25, ny=17, nvrt=10)
+    mix = Model([a, b, d])
+    mix.step(6)
+    for k, c in enumerate([a, b, d]):
+        alone = Model([c])
+        alone.step(6)
+        for f in ("ETA2", "SIDE_U2", "ELEM_TR", "NODE_U2"):
+            assert np.array_equal(mix.get(k, f), alone.get(0, f)), (k, f)
+        assert mix.stats(k)["jcg_iters"] == alone.stats(0)["jcg_iters"]
+        alone.close()
+
+
+def test_mixed_precision_elevation_within_1e6_m(native, oracle_lib):
+    """FP32 inner JCG with FP64 refinement: elevation within 1e-6 m of the FP64 oracle."""
+    from gschism_b200.model import Model
+    from oracle.step_api import OracleModel
+    c = cases.channel(seed=4)
+    o = OracleModel(c)
+    g = Model([c], precision="fp32_ir")
+    n = 20
+    o.run(n)
+    g.step(n)
+    err = np.abs(g.get(0, "ETA2") - o.get("ETA2")).max()
+    assert err <= 1e-6, err
+    st = g.stats(0)
+    assert st["jcg_outer"] >= 1
