@@ -74,11 +74,13 @@ __device__ __forceinline__ bool grid_sync(unsigned* count, unsigned* gen, int32_
             __threadfence();
             atomicAdd(gen, 1u);
         } else {
+            // tight polling first (the common case: every block arrives within microseconds),
+            // then back off; about 2 s in total before the wait is declared failed
             long long spins = 0;
             while (*vgen == g) {
-                __nanosleep(64);
-                if (++spins > (1ll << 25)) { atomicOr(err, ERR_BARRIER_TIMEOUT); break; }
-                if (*((volatile int32_t*)err) & ERR_BARRIER_TIMEOUT) break;
+                if (++spins > 4096) __nanosleep(128);
+                if (spins > (1ll << 24)) { atomicOr(err, ERR_BARRIER_TIMEOUT); break; }
+                if ((spins & 255) == 0 && (*((volatile int32_t*)err) & ERR_BARRIER_TIMEOUT)) break;
             }
         }
         __threadfence();
