@@ -94,3 +94,28 @@ def test_product_rejects_broken_mesh(native):
     P = lambda a: a.ctypes.data_as(L.PI)
     assert native.gs_grid_build(np_, ne, P(np.ascontiguousarray(el4.ravel())), P(i34), P(isb),
                                 *[P(a) for a in out]) == L.GS_ERR_BAD_MESH
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_readhgrid_shim_matches_reference_tuple(name, gcases, tmp_path, native):
+    """gschism_b200.grid.readHGrid returns the reference's tuple on the same hgrid.gr3."""
+    from gschism_b200 import grid
+    g = _gold(name)
+    c = gcases[name]
+    cases.write_case(c, str(tmp_path))
+    out = grid.readHGrid(str(tmp_path / "hgrid.gr3"), "", 1, 0)
+    names = ["i34", "partElements", "partNodes", "partSides", "elnode", "elside", "nodeCoords", "nodeCoords_ll",
+             "ic3", "isdel", "isidenode", "isbnd", "nond", "nlnd", "iond", "ilnd"]
+    for k, nm in enumerate(names):
+        if nm == "nodeCoords_ll":
+            continue
+        np.testing.assert_array_equal(np.asarray(out[k]), g[nm], err_msg=nm)
+    for k, nm in ((16, "nodeNeighElems"), (17, "nodeNeighNodes")):
+        np.testing.assert_array_equal(out[k][0], g[nm + "_data"])
+        np.testing.assert_array_equal(out[k][1], g[nm + "_start"])
+    v = grid.readVGrid(str(tmp_path / "vgrid.in"), c.n_nodes)
+    np.testing.assert_array_equal(v[0], g["vgrid_ints"])
+    np.testing.assert_array_equal(v[1], g["vgrid_ztot"])
+    np.testing.assert_array_equal(v[3], g["vgrid_params"])
+    np.testing.assert_array_equal(v[5], g["vgrid_sigma"])
+    np.testing.assert_allclose(v[6], g["vgrid_cs"], rtol=0, atol=1e-15)
