@@ -25,7 +25,7 @@ PHASE = dict(BEGIN=0, BTRACK=1, PREPARE=2, ASSEMBLE=3, SOLVE=4, UPDATE_ELEV=5, M
 EXPORTS = ["gs_grid_build", "gs_ctx_create", "gs_member_add", "gs_ctx_finalize", "gs_ctx_destroy",
            "gs_last_error", "gs_sync", "gs_set_stream", "gs_step", "gs_phase", "gs_state_get", "gs_state_put", "gs_set_tau",
            "gs_get_stats", "gs_member_sizes", "gs_jcg_create", "gs_jcg_buffers", "gs_jcg_solve_csr",
-           "gs_jcg_check", "gs_jcg_destroy", "gs_jcg_last_error"]
+           "gs_jcg_check", "gs_jcg_destroy", "gs_jcg_last_error", "gs_jcg_solve_csr_noalloc"]
 
 
 class GsConfig(ctypes.Structure):
@@ -95,6 +95,8 @@ def load(build_if_missing: bool = False):
     L.gs_jcg_destroy.argtypes = [c_void_p]
     L.gs_jcg_last_error.argtypes = [c_void_p]
     L.gs_jcg_last_error.restype = ctypes.c_char_p
+    L.gs_jcg_solve_csr_noalloc.argtypes = [I, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double, I, I,
+                                           c_void_p, ctypes.POINTER(c_int)]
     for name in EXPORTS:
         if name not in ("gs_last_error", "gs_jcg_last_error"):
             getattr(L, name).restype = c_int

@@ -16,6 +16,9 @@
 //   B: alpha = rz/p.q; x += alpha p; r -= alpha q; z = invD r; r.r and r.z partials.
 // GS_FP32_IR runs the same iteration in FP32 (FP32 matrix copy and vectors, FP64 dot products)
 // on the residual equation A d = r inside FP64 refinement sweeps r = b - A x, x += d.
+#include <algorithm>
+#include <mutex>
+
 #include "dev_common.cuh"
 #include "kernels.h"
 
@@ -583,4 +586,123 @@ cudaError_t jcg_read_iters(JcgWork* w, std::vector<int>& iters, std::vector<int>
 
 int32_t* jcg_iters_device(JcgWork* w) { return w->mdone; }
 
+// ------------------------------------------------------------- solve without allocating ----
+//
+// gs_jcg_solve_csr_noalloc: the FP64 solve of k_jcg64 on a caller CSR for callers that cannot
+// allocate device memory.  Its scratch (residual, search directions, inverse diagonal, tile
+// partials, tile tables and control words) lives in the file-scope array below; every GPU that
+// loads the library holds it until the process exits.
+
+constexpr int kNoAllocMaxRows = 65536;
+constexpr int kNoAllocTileRows = 256;
+constexpr int kNoAllocMaxTiles = kNoAllocMaxRows / kNoAllocTileRows;     // 256
+constexpr int kNoAllocMaxBlocks = kNoAllocMaxTiles;
+// byte offsets inside the scratch array (all 256-byte aligned)
+constexpr size_t kNaVec = sizeof(double) * kNoAllocMaxRows;              // one FP64 vector
+constexpr size_t kNaOffPart = 6 * kNaVec;
+constexpr size_t kNaOffAtol = kNaOffPart + sizeof(double) * R_KINDS * kNoAllocMaxTiles;
+constexpr size_t kNaOffTiles = kNaOffAtol + 256;
+constexpr size_t kNaOffBlk = kNaOffTiles + 3 * sizeof(int32_t) * kNoAllocMaxTiles;
+constexpr size_t kNaOffCtl = kNaOffBlk + sizeof(int32_t) * (kNoAllocMaxBlocks + 64);
+constexpr size_t kNaCtlBytes = 256;
+constexpr size_t kNoAllocBytes = kNaOffCtl + kNaCtlBytes;                // about 3.1 MiB
+
+static __device__ __align__(256) unsigned char gs_noalloc_scratch[kNoAllocBytes];
+
+// control words at kNaOffCtl: [0] mem_t0, [1] mem_t1, [2] mdone, [3] mouter, [4] ndone,
+// [5] bar_count, [6] bar_gen, [7] err
+
+__global__ void k_noalloc_setup(unsigned char* base, int n, const int32_t* indptr, const int32_t* indices,
+                                const double* A, int ntiles, int grid) {
+    // tile tables of one member, block ranges, cleared control words, inverse diagonal
+    int32_t* tr0 = (int32_t*)(base + kNaOffTiles);
+    int32_t* tr1 = tr0 + kNoAllocMaxTiles;
+    int32_t* tm = tr1 + kNoAllocMaxTiles;
+    int32_t* bt = (int32_t*)(base + kNaOffBlk);
+    int32_t* ctl = (int32_t*)(base + kNaOffCtl);
+    double* invD = (double*)(base + 5 * kNaVec);
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x, G = gridDim.x * blockDim.x;
+    for (int t = gid; t < ntiles; t += G) {
+        tr0[t] = t * kNoAllocTileRows;
+        tr1[t] = min(n, (t + 1) * kNoAllocTileRows);
+        tm[t] = 0;
+    }
+    for (int b = gid; b <= grid; b += G) bt[b] = (int32_t)((long long)ntiles * b / grid);
+    if (gid < (int)(kNaCtlBytes / 4)) ctl[gid] = (gid == 1) ? ntiles : (gid == 2 ? -1 : 0);
+    for (int i = gid; i < n; i += G) {
+        double dg = 0.0;
+        for (int a = indptr[i]; a < indptr[i + 1]; a++)
+            if (indices[a] == i) dg = A[a];
+        invD[i] = 1.0 / dg;
+    }
+}
+
+static std::mutex g_noalloc_mu;
+static unsigned char* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array on the current device, looked up once per device.
+static cudaError_t noalloc_base(unsigned char** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, gs_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = (unsigned char*)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace gs
+
+extern "C" gs_status gs_jcg_solve_csr_noalloc(int n, const int32_t* indptr, const int32_t* indices,
+                                              const double* data, const double* b, double* x, double rtol,
+                                              int maxiter, int check_every, void* stream, int* iters) {
+    using namespace gs;
+    if (n <= 0 || n > kNoAllocMaxRows || !indptr || !indices || !data || !b || !x || maxiter < 1)
+        return GS_ERR_ARG;
+    unsigned char* base = nullptr;
+    if (noalloc_base(&base) != cudaSuccess) return GS_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int ntiles = (n + kNoAllocTileRows - 1) / kNoAllocTileRows;
+    const int grid = std::max(1, std::min(ntiles, coop_blocks((const void*)k_jcg64, nsm)));
+    k_noalloc_setup<<<std::max(1, std::min(64, (n + 255) / 256)), 256, 0, st>>>(base, n, indptr, indices, data,
+                                                                               ntiles, grid);
+    int32_t* ctl = (int32_t*)(base + kNaOffCtl);
+    JcgView J{};
+    J.n = n; J.nmem = 1; J.ntiles = ntiles;
+    J.indptr = indptr; J.indices = indices; J.A = data; J.b = b; J.x = x;
+    J.r = (double*)(base + 0 * kNaVec); J.z = (double*)(base + 1 * kNaVec); J.q = (double*)(base + 2 * kNaVec);
+    J.p0 = (double*)(base + 3 * kNaVec); J.p1 = (double*)(base + 4 * kNaVec);
+    J.invD = (const double*)(base + 5 * kNaVec);
+    J.tile_part = (double*)(base + kNaOffPart);
+    J.mem_atol2 = (double*)(base + kNaOffAtol);
+    J.tile_r0 = (const int32_t*)(base + kNaOffTiles);
+    J.tile_r1 = J.tile_r0 + kNoAllocMaxTiles;
+    J.tile_mem = J.tile_r1 + kNoAllocMaxTiles;
+    J.blk_t0 = (const int32_t*)(base + kNaOffBlk);
+    J.mem_t0 = ctl + 0; J.mem_t1 = ctl + 1; J.mdone = ctl + 2; J.mouter = ctl + 3;
+    J.ndone = (unsigned*)(ctl + 4); J.bar_count = (unsigned*)(ctl + 5); J.bar_gen = (unsigned*)(ctl + 6);
+    J.err = ctl + 7;
+    J.rtol = rtol; J.maxiter = maxiter; J.check_every = check_every > 0 ? check_every : 1;
+    void* args[] = {&J};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_jcg64, dim3(grid), dim3(kThreads), args, 0, st);
+    if (e != cudaSuccess) return GS_ERR_CUDA;
+    int32_t h[8] = {0};
+    e = cudaMemcpyAsync(h, ctl, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return GS_ERR_CUDA;
+    if (iters) *iters = h[2];
+    if (h[7] & ERR_BARRIER_TIMEOUT) return GS_ERR_TIMEOUT;
+    return GS_OK;
+}
+
+namespace gs {
 }  // namespace gs

@@ -167,6 +167,22 @@ gs_status gs_jcg_check(gs_jcg* s, double* relres);
 gs_status gs_jcg_destroy(gs_jcg* s);
 const char* gs_jcg_last_error(const gs_jcg* s);
 
+/* FP64 JCG on a caller CSR that allocates no device memory.  No counterpart in the reference.
+ * For callers that cannot allocate: a host whose device memory is entirely handed out by its own
+ * pool, or a loop that must not pay allocation latency mid-run.  Every argument except iters is
+ * a device pointer the caller owns; x holds the initial guess on entry and the solution on exit
+ * (no solution history is kept).  Same rules as gs_jcg_solve_csr: atol = rtol*|b|, test every
+ * check_every iterations, *iters = maxiter when the tolerance is not met.  The work space is a
+ * fixed array inside the library (about 3.1 MiB on every GPU that loads it, kept until the
+ * process exits), so n is limited to 65536 rows; larger n returns GS_ERR_ARG.  The first call on
+ * a device looks up that array's device address (a one-time set-up per device); that first call
+ * should come before any stream capture.  All calls share the array: calls that overlap in time
+ * on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller.  stream may be NULL. */
+gs_status gs_jcg_solve_csr_noalloc(int n, const int32_t* indptr, const int32_t* indices, const double* data,
+                                   const double* b, double* x, double rtol, int maxiter, int check_every,
+                                   void* stream, int* iters);
+
 #ifdef __cplusplus
 }
 #endif
