@@ -59,29 +59,32 @@ __device__ __forceinline__ double2 clampvel(double2 v, double rmaxvel) {
     return v2(fmin(fmax(v.x, -rmaxvel), rmaxvel), fmin(fmax(v.y, -ry), ry));
 }
 
-// Grid-wide barrier for cooperative launches.  The wait is bounded: after ~2 s of polling the
-// block records ERR_BARRIER_TIMEOUT and returns false, and every caller then leaves the kernel.
-__device__ __forceinline__ bool grid_sync(unsigned* count, unsigned* gen, int32_t* err) {
+// Grid-wide barrier for cooperative launches on one 32-bit word that starts at zero.  Each
+// block adds 1, except block 0, which adds 2^31 - (blocks - 1): the increments of one round sum
+// to 2^31, so the word's top bit flips exactly when the last block arrives and the low bits are
+// back at zero for the next round.  A waiting block polls until the top bit differs from the one
+// its own add returned: one atomic per block and no reset store.  The wait is bounded: after
+// about 2 s of polling the block records ERR_BARRIER_TIMEOUT and returns false, and every caller
+// then leaves the kernel (the host clears the word before the next launch).
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ bool grid_sync(unsigned* bar, int32_t* err) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
-        volatile unsigned* vgen = gen;
-        const unsigned g = *vgen;
+        const bool first = (blockIdx.x | blockIdx.y | blockIdx.z) == 0;
+        const unsigned inc = first ? (0x80000000u - (nb - 1u)) : 1u;
         __threadfence();
-        const unsigned arrived = atomicAdd(count, 1u);
-        if (arrived == nb - 1) {
-            *count = 0;
-            __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
-            // tight polling first (the common case: every block arrives within microseconds),
-            // then back off; about 2 s in total before the wait is declared failed
-            long long spins = 0;
-            while (*vgen == g) {
-                if (++spins > 4096) __nanosleep(128);
-                if (spins > (1ll << 24)) { atomicOr(err, ERR_BARRIER_TIMEOUT); break; }
-                if ((spins & 255) == 0 && (*((volatile int32_t*)err) & ERR_BARRIER_TIMEOUT)) break;
-            }
+        const unsigned old = atomicAdd(bar, inc);
+        long long spins = 0;
+        while (((ld_acquire_u32(bar) ^ old) & 0x80000000u) == 0u) {
+            if (++spins > 4096) __nanosleep(128);
+            if (spins > (1ll << 24)) { atomicOr(err, ERR_BARRIER_TIMEOUT); break; }
+            if ((spins & 255) == 0 && (*((volatile int32_t*)err) & ERR_BARRIER_TIMEOUT)) break;
         }
         __threadfence();
     }

@@ -22,6 +22,7 @@ constexpr int kMaxTracers = 8;
 constexpr int kMaxLevels = 64;
 constexpr int kMaxBfr = 8;
 constexpr int kMaxDeg = 24;        // max node degree supported by the per-row assembly
+constexpr int kIrVectors = 10;     // FP32 vectors of the refinement solve: (u, w, s, -) x 2, p, d
 
 // Device error bits (gs_stats.error_flags)
 enum : int {
@@ -56,12 +57,17 @@ struct Dev {
     int32_t *bn_node, *bn_ietype, *bn_nbfr;
     double *bn_emo, *bn_efa, *bn_amig, *bn_ff, *bn_face;   // [NB][kMaxBfr]
     // CSR of the elevation matrix (rows = nodes)
-    int32_t *indptr, *indices;
+    // elevation matrix (rows = nodes) in SELL-32 layout: slices of 32 consecutive rows; entry k
+    // of row i sits at sell[i/32].x + 32*k + i%32 for k < sell[i/32].y (the slice's widest row).
+    // A row's entries are in increasing column order; padding entries hold the row's own column
+    // and a zero value.
+    int2* sell;
+    int32_t *indices;
     double *A;
-    float *A32;
+    float *A32;                    // D^-1 A in FP32 (refinement solve)
     // JCG vectors
     double *b, *xs, *r, *zz, *p0, *p1, *q, *invD, *xh0, *xh1, *xh2;
-    float *r32, *z32, *p032, *p132, *q32, *d32, *invD32;
+    float *ir32, *diag32;          // ir32: kIrVectors FP32 vectors of the refinement solve
     // sides
     int32_t *sn, *se;              // [2][NS]
     double *len, *snx, *sny, *scx, *scy, *cori;
@@ -97,7 +103,7 @@ struct Dev {
     double *mem_scal;              // per member scalars (see jcg.cu)
     int32_t *mem_iters, *mem_outer;
     // global control
-    unsigned *bar_count, *bar_gen;
+    unsigned* bar;                  // grid barrier word (zero between launches)
     int32_t *err;
     unsigned long long *counters;  // [4]: walk cap hits, btrack stops, ...
 };

@@ -10,12 +10,13 @@
 // bit-identical results alone and inside any batch.  Scalars stay on the device; convergence is
 // tested every check_every iterations on the device, so a solve never returns to the host.
 //
-// Per iteration two phases separated by grid barriers:
+// GS_FP64: per iteration two phases separated by grid barriers:
 //   A: beta = rz/rz_old; p_new = z + beta p; q = A p_new (p_new of neighbour rows is formed on
 //      the fly from z and the previous p, so no barrier is needed between p and q); p.q partials
 //   B: alpha = rz/p.q; x += alpha p; r -= alpha q; z = invD r; r.r and r.z partials.
-// GS_FP32_IR runs the same iteration in FP32 (FP32 matrix copy and vectors, FP64 dot products)
-// on the residual equation A d = r inside FP64 refinement sweeps r = b - A x, x += d.
+// GS_FP32_IR solves the residual equation A d = r in FP32 (FP32 matrix and vectors, FP64 dot
+// products) inside FP64 refinement sweeps r = b - A x, x += d, with the single-reduction form of
+// the iteration (one barrier per iteration; see k_jcg_ir).
 #include <algorithm>
 #include <mutex>
 
@@ -26,24 +27,29 @@ namespace gs {
 
 constexpr int kThreads = 256;
 
-enum { R_BB = 0, R_PQ = 1, R_RR0 = 2, R_RZ0 = 3, R_RR1 = 4, R_RZ1 = 5, R_OUT = 6, R_KINDS = 7 };
+enum { R_BB = 0, R_PQ = 1, R_RR0 = 2, R_RZ0 = 3, R_RR1 = 4, R_RZ1 = 5, R_OUT = 6, R_WU0 = 7, R_WU1 = 8, R_KINDS = 9 };
 
 struct JcgView {
     int n, nmem, ntiles;
-    const int32_t *indptr, *indices;
+    const int32_t *indptr, *indices;   // CSR rows (indptr), or SELL-32 slices when sell is set
+    const int2* sell;
     const double* A;
-    const float* A32;
+    const float* A32;              // D^-1 A in FP32 (refinement solve)
     const double* b;
     const double* invD;
     double *x, *r, *z, *q, *p0, *p1;
-    float *r32, *z32, *q32, *p032, *p132, *d32, *invD32;
+    float* ir32;                   // kIrVectors FP32 vectors of the refinement solve
+    const float* diag32;           // D in FP32
     const int32_t *tile_r0, *tile_r1, *tile_mem, *mem_t0, *mem_t1, *blk_t0;   // blk_t0: [grid+1]
     double* tile_part;             // [R_KINDS][ntiles]
     double* mem_atol2;             // [nmem]
     int32_t* mdone;                // [nmem] iterations at convergence, -1 while active
     int32_t* mouter;               // [nmem] refinement sweeps (IR)
+    int32_t* minner;               // [nmem] inner iterations so far (IR)
+    int32_t* mret;                 // [nmem] inner iteration at which the sweep's solve finished, -1 before
+    double* mem_ab;                // [4][nmem] alpha (parity 0, 1) and gamma (parity 0, 1) of the inner solve
     unsigned* ndone;
-    unsigned *bar_count, *bar_gen;
+    unsigned* bar;
     int32_t* err;
     double rtol;
     int maxiter, check_every;
@@ -107,6 +113,48 @@ __device__ __forceinline__ int uniform_ld(const int32_t* p, int* shv) {
     return *shv;
 }
 
+// Entries of row i: positions off + k * stride for k < n, in increasing column order.
+struct RowRange { int off, n, stride; };
+
+template <bool SELL>
+__device__ __forceinline__ RowRange row_range(const JcgView& J, int i) {
+    if constexpr (SELL) {
+        const int2 sw = __ldg(J.sell + (i >> 5));
+        return {sw.x + (i & 31), sw.y, 32};
+    } else {
+        const int a0 = __ldg(J.indptr + i), a1 = __ldg(J.indptr + i + 1);
+        return {a0, a1 - a0, 1};
+    }
+}
+
+// Row product sum_k vals[e_k] * g(indices[e_k]) over the row's entries e_k, in entry order.
+// Entries are fetched eight at a time and all index and value loads of a chunk are issued before
+// its gathers, so a row of up to eight entries costs about two memory latencies rather than two
+// per entry.  Slots past the row's end gather the row itself with a zero weight, which leaves the
+// sum unchanged.  In SELL-32 layout the loads of one slot are contiguous across a warp.
+template <bool SELL, typename T, typename G>
+__device__ __forceinline__ T row_dot(const JcgView& J, const T* __restrict__ vals, int i, G g) {
+    const RowRange rr = row_range<SELL>(J, i);
+    T s = (T)0;
+    for (int base = 0; base < rr.n; base += 8) {
+        int c[8];
+        T v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const bool ok = base + k < rr.n;
+            const int e = rr.off + (base + k) * rr.stride;
+            c[k] = ok ? __ldg(J.indices + e) : i;
+            v[k] = ok ? __ldg(vals + e) : (T)0;
+        }
+        T gv[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) gv[k] = g(c[k]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) s += v[k] * gv[k];
+    }
+    return s;
+}
+
 __device__ __forceinline__ bool checkpoint(const JcgView& J, int it, int maxit) {
     return ((it + 1) % J.check_every == 0) || (it == maxit - 1);
 }
@@ -116,7 +164,7 @@ __device__ __forceinline__ bool checkpoint(const JcgView& J, int it, int maxit) 
 // Phase A of CG iteration `it` on the tiles of this block.  T = double (FP64 solve) or float
 // (inner solve of the refinement).  Members whose iteration it-1 met the tolerance at a
 // checkpoint are retired here (the member's first tile records the count).
-template <typename T>
+template <bool SELL, typename T>
 __device__ void cg_phase_a(const JcgView& J, int it, int maxit, const T* A, const T* z, T* pc, T* pn, T* q,
                            double* sh, int* shv) {
     const int tid = threadIdx.x;
@@ -147,12 +195,7 @@ __device__ void cg_phase_a(const JcgView& J, int it, int maxit, const T* A, cons
         double v[1] = {0.0};
         const T bt = (T)beta;
         for (int i = r0 + tid; i < r1; i += kThreads) {
-            T s = (T)0;
-            const int a1 = J.indptr[i + 1];
-            for (int a = J.indptr[i]; a < a1; a++) {
-                const int c = J.indices[a];
-                s += A[a] * (z[c] + bt * pc[c]);
-            }
+            const T s = row_dot<SELL, T>(J, A, i, [&](int c) { return z[c] + bt * pc[c]; });
             const T pi = z[i] + bt * pc[i];
             pn[i] = pi; q[i] = s;
             v[0] += (double)pi * (double)s;
@@ -235,10 +278,11 @@ __device__ void phase_atol(const JcgView& J, double* sh) {
     }
 }
 
-#define GSYNC() do { if (!grid_sync(J.bar_count, J.bar_gen, J.err)) return; } while (0)
+#define GSYNC() do { if (!grid_sync(J.bar, J.err)) return; } while (0)
 
 // ------------------------------------------------------------------------------- FP64 ----
 
+template <bool SELL>
 __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
     __shared__ double sh[4 * 32];
     __shared__ int shv;
@@ -256,8 +300,7 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
             double v[2] = {0.0, 0.0};
             for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
                 if (zero) { J.x[i] = 0.0; J.r[i] = 0.0; J.z[i] = 0.0; continue; }
-                double s = 0.0;
-                for (int a = J.indptr[i]; a < J.indptr[i + 1]; a++) s += J.A[a] * J.x[J.indices[a]];
+                const double s = row_dot<SELL, double>(J, J.A, i, [&](int c) { return J.x[c]; });
                 const double ri = J.b[i] - s, zi = J.invD[i] * ri;
                 J.r[i] = ri; J.z[i] = zi;
                 v[0] += ri * ri; v[1] += ri * zi;
@@ -271,7 +314,7 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
     for (; it < J.maxiter; it++) {
         double* pc = (it & 1) ? J.p1 : J.p0;
         double* pn = (it & 1) ? J.p0 : J.p1;
-        cg_phase_a<double>(J, it, J.maxiter, J.A, J.z, pc, pn, J.q, sh, &shv);
+        cg_phase_a<SELL, double>(J, it, J.maxiter, J.A, J.z, pc, pn, J.q, sh, &shv);
         GSYNC();
         if (*((volatile unsigned*)J.ndone) >= (unsigned)J.nmem) break;
         cg_phase_b<double>(J, it, J.maxiter, J.x, J.r, J.z, pn, J.q, J.invD, sh, &shv);
@@ -291,175 +334,201 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
 }
 
 // ---------------------------------------------------------------------- FP32 + refinement ----
+//
+// Outer FP64 sweeps r = b - A x, x += d around an inner FP32 solve of A d = r.  The inner solve is
+// the single-reduction form of Jacobi-PCG (Chronopoulos and Gear, 1989): with u = D^-1 r and
+// w = A u the recurrences
+//   s_i = w_i + beta_i s_{i-1},   p_i = u_i + beta_i p_{i-1},   d += alpha_i p_i,
+//   r_{i+1} = r_i - alpha_i s_i,  w_{i+1} = A u_{i+1},
+//   gamma = (r, u), delta = (w, u),  beta_i = gamma_i / gamma_{i-1},
+//   alpha_i = gamma_i / (delta_i - beta_i gamma_i / alpha_{i-1})
+// give the iterates of the two-reduction loop with one grid-wide reduction per iteration.  The
+// vectors are kept scaled by D^-1 (u, w~ = D^-1 w, s~ = D^-1 s) and the FP32 matrix copy holds
+// D^-1 A, so u_{i+1} = u_i - alpha_i s~_i and w~_{i+1} = (D^-1 A) u_{i+1}; the dot products use
+// the FP32 diagonal D: gamma = sum D u^2, delta = sum D w~ u, r.r = sum (D u)^2.  A row's
+// w~_{i+1} needs u_{i+1} of its neighbours; each block forms those on the fly from the neighbours'
+// (u_i, w~_i, s~_{i-1}), so u, w~ and s~ are double-buffered by iteration parity and no barrier
+// separates the vector update from the matrix product.
 
+// FP32 vectors in ir32: (u, w~, s~, unused) packed per row for iteration parities 0 and 1
+// (4 n floats each, so a neighbour's three values arrive in one 16-byte load), then p and d.
+static_assert(kIrVectors == 10, "ir32 layout");
+__device__ __forceinline__ float4* ir_uws(const JcgView& J, int parity) {
+    return reinterpret_cast<float4*>(J.ir32) + (size_t)parity * J.n;
+}
+__device__ __forceinline__ float* ir_p(const JcgView& J) { return J.ir32 + (size_t)8 * J.n; }
+__device__ __forceinline__ float* ir_d(const JcgView& J) { return J.ir32 + (size_t)9 * J.n; }
+
+// u_{i+1} of a row from its (u_i, w~_i, s~_{i-1}); the same expression for a row and its neighbours
+__device__ __forceinline__ float u_next(float4 q, float al, float bt) { return q.x - al * (q.y + bt * q.z); }
+
+__device__ __forceinline__ int ld_i32(const int32_t* p) { return *((const volatile int32_t*)p); }
+
+// a member takes part in inner iteration it unless it retired before it (mret is written once
+// per sweep, with the iteration at which the member met the inner tolerance, during that very
+// iteration; both values a block may read then lead to the same decision)
+__device__ __forceinline__ bool inner_member_on(const JcgView& J, int m, int it) {
+    if (ld_i32(&J.mdone[m]) >= 0 || ld_i32(&J.mouter[m]) <= 0) return false;
+    const int r = ld_i32(&J.mret[m]);
+    return r < 0 || r >= it;
+}
+
+template <bool SELL>
 __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
     __shared__ double sh[4 * 32];
     __shared__ int shv;
     const int tid = threadIdx.x;
     const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
+    const int nmem = J.nmem;
+    float* const pp = ir_p(J);
+    float* const dd = ir_d(J);
     phase_bb(J, sh);
     GSYNC();
     phase_atol(J, sh);
     GSYNC();
-    int total_inner = 0;
     for (int outer = 0; outer < 64; outer++) {
-        // O1: FP64 residual r = b - A x, outer r.r partials, FP32 copies, d = 0
-        for (int t = tb0; t < tb1; t++) {
-            const int m = J.tile_mem[t];
-            const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
-            const int dn = uniform_ld(&J.mdone[m], &shv);
-            if (dn >= 0) {
-                if (outer == 0 && dn == 0)
-                    for (int i = r0 + tid; i < r1; i += kThreads) J.x[i] = 0.0;
-                continue;
-            }
-            double v[1] = {0.0};
-            for (int i = r0 + tid; i < r1; i += kThreads) {
-                double s = 0.0;
-                for (int a = J.indptr[i]; a < J.indptr[i + 1]; a++) s += J.A[a] * J.x[J.indices[a]];
-                const double ri = J.b[i] - s;
-                J.r32[i] = (float)ri; J.d32[i] = 0.0f; J.p032[i] = 0.0f; J.p132[i] = 0.0f;
-                v[0] += ri * ri;
-            }
-            const int kinds[1] = {R_OUT};
-            put_partials<1>(J, t, kinds, v, sh);
-        }
-        GSYNC();
-        // O2: outer convergence test; inner start z = invD r, (r.r, r.z) of the FP32 residual
-        for (int t = tb0; t < tb1; t++) {
-            const int m = J.tile_mem[t];
-            if (uniform_ld(&J.mdone[m], &shv) >= 0) continue;
-            const int kinds1[1] = {R_OUT};
-            double tot[1];
-            member_totals<1>(J, m, kinds1, tot, sh);
-            if (tot[0] <= J.mem_atol2[m]) {
-                if (t == J.mem_t0[m] && tid == 0) {
-                    J.mdone[m] = total_inner; J.mouter[m] = outer;
-                    __threadfence(); atomicAdd(J.ndone, 1u);
+        // O1: FP64 residual r = b - A x; u_0 = D^-1 r in FP32; s~, p, d = 0; outer r.r partials
+        {
+            float4* uw0 = ir_uws(J, 0);
+            for (int t = tb0; t < tb1; t++) {
+                const int m = J.tile_mem[t];
+                const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
+                const int dn = uniform_ld(&J.mdone[m], &shv);
+                if (dn >= 0) {
+                    if (outer == 0 && dn == 0)
+                        for (int i = r0 + tid; i < r1; i += kThreads) J.x[i] = 0.0;
+                    continue;
                 }
-                continue;
+                double v[1] = {0.0};
+                for (int i = r0 + tid; i < r1; i += kThreads) {
+                    const double s = row_dot<SELL, double>(J, J.A, i, [&](int c) { return J.x[c]; });
+                    const double ri = J.b[i] - s;
+                    uw0[i] = make_float4((float)(J.invD[i] * ri), 0.0f, 0.0f, 0.0f);
+                    pp[i] = 0.0f; dd[i] = 0.0f;
+                    v[0] += ri * ri;
+                }
+                const int kinds[1] = {R_OUT};
+                put_partials<1>(J, t, kinds, v, sh);
             }
-            if (t == J.mem_t0[m] && tid == 0) { J.mem_atol2[J.nmem + m] = J.inner_rtol * J.inner_rtol * tot[0]; J.mouter[m] = outer + 1; }
-            const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
-            double v[2] = {0.0, 0.0};
-            for (int i = r0 + tid; i < r1; i += kThreads) {
-                const float ri = J.r32[i], zi = J.invD32[i] * ri;
-                J.z32[i] = zi;
-                v[0] += (double)ri * (double)ri; v[1] += (double)ri * (double)zi;
-            }
-            const int kinds[2] = {R_RR1, R_RZ1};
-            put_partials<2>(J, t, kinds, v, sh);
         }
         GSYNC();
-        if (*((volatile unsigned*)J.ndone) >= (unsigned)J.nmem) break;
-        // inner FP32 JCG on A d = r: a member leaves when its inner r.r <= inner_rtol^2 * outer r.r
-        // (tested at checkpoints); its mdone stays -1, so the inner loop tracks retirement by
-        // the per-sweep marker in mouter (negative once the member's inner solve has finished)
+        // O2: outer convergence test; w~_0 = (D^-1 A) u_0 and (gamma, delta, r.r) of iteration 0
+        {
+            float4* uw0 = ir_uws(J, 0);
+            const float* u0 = J.ir32;          // u components of parity 0 (stride 4)
+            for (int t = tb0; t < tb1; t++) {
+                const int m = J.tile_mem[t];
+                if (uniform_ld(&J.mdone[m], &shv) >= 0) continue;
+                const int kinds1[1] = {R_OUT};
+                double tot[1];
+                member_totals<1>(J, m, kinds1, tot, sh);
+                const bool owner = (t == J.mem_t0[m] && tid == 0);
+                if (tot[0] <= J.mem_atol2[m]) {
+                    if (owner) {
+                        J.mdone[m] = J.minner[m]; J.mouter[m] = outer;
+                        __threadfence(); atomicAdd(J.ndone, 1u);
+                    }
+                    continue;
+                }
+                if (owner) {
+                    J.mem_atol2[nmem + m] = J.inner_rtol * J.inner_rtol * tot[0];
+                    J.mouter[m] = outer + 1;
+                    J.mret[m] = -1;
+                }
+                const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
+                double v[3] = {0.0, 0.0, 0.0};
+                for (int i = r0 + tid; i < r1; i += kThreads) {
+                    // neighbours read only the u component, this row writes only its w~ component
+                    const float w = row_dot<SELL, float>(J, J.A32, i, [&](int c) { return u0[4 * (size_t)c]; });
+                    uw0[i].y = w;
+                    const double ui = u0[4 * (size_t)i], dg = J.diag32[i], du = dg * ui;
+                    v[0] += du * ui; v[1] += dg * (double)w * ui; v[2] += du * du;
+                }
+                const int kinds[3] = {R_RZ0, R_WU0, R_RR0};
+                put_partials<3>(J, t, kinds, v, sh);
+            }
+        }
+        GSYNC();
+        if (*((volatile unsigned*)J.ndone) >= (unsigned)nmem) break;
         int it = 0;
         for (; it < J.inner_maxiter; it++) {
-            float* pc = (it & 1) ? J.p132 : J.p032;
-            float* pn = (it & 1) ? J.p032 : J.p132;
-            // inner retirement uses the same parity slots; members with mouter < 0 are skipped
-            {
-                const int cur = (it + 1) & 1, old = it & 1;
-                int cm = -1;
-                bool active = false;
-                double beta = 0.0;
-                for (int t = tb0; t < tb1; t++) {
-                    const int m = J.tile_mem[t];
-                    if (m != cm) {
-                        cm = m;
-                        active = uniform_ld(&J.mdone[m], &shv) < 0 && uniform_ld(&J.mouter[m], &shv) > 0;
-                        if (active) {
-                            const int kinds[3] = {cur ? R_RR1 : R_RR0, cur ? R_RZ1 : R_RZ0, old ? R_RZ1 : R_RZ0};
-                            double tot[3];
-                            member_totals<3>(J, m, kinds, tot, sh);
-                            if (it > 0 && checkpoint(J, it - 1, J.inner_maxiter) && tot[0] <= J.mem_atol2[J.nmem + m]) {
-                                active = false;
-                                if (t == J.mem_t0[m] && tid == 0) J.mouter[m] = -J.mouter[m];
-                            } else {
-                                beta = (it == 0 || tot[2] == 0.0) ? 0.0 : tot[1] / tot[2];
-                            }
-                        }
-                    }
-                    if (!active) continue;
-                    const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
-                    const float bt = (float)beta;
-                    double v[1] = {0.0};
-                    for (int i = r0 + tid; i < r1; i += kThreads) {
-                        float s = 0.0f;
-                        for (int a = J.indptr[i]; a < J.indptr[i + 1]; a++) {
-                            const int c = J.indices[a];
-                            s += J.A32[a] * (J.z32[c] + bt * pc[c]);
-                        }
-                        const float pi = J.z32[i] + bt * pc[i];
-                        pn[i] = pi; J.q32[i] = s;
-                        v[0] += (double)pi * (double)s;
-                    }
-                    const int kinds[1] = {R_PQ};
-                    put_partials<1>(J, t, kinds, v, sh);
-                }
-            }
-            GSYNC();
-            // every member finished its inner solve -> leave the inner loop (uniform decision)
             bool any = false;
-            for (int m = 0; m < J.nmem && !any; m++)
-                any = ld_done(J, m) < 0 && *((volatile int32_t*)&J.mouter[m]) > 0;
+            for (int m = 0; m < nmem && !any; m++) any = inner_member_on(J, m, it);
             if (!any) break;
-            {
-                const int cur = (it + 1) & 1;
-                const int srr = (it & 1) ? R_RR1 : R_RR0, srz = (it & 1) ? R_RZ1 : R_RZ0;
-                int cm = -1;
-                bool active = false;
-                double alpha = 0.0;
-                for (int t = tb0; t < tb1; t++) {
-                    const int m = J.tile_mem[t];
-                    if (m != cm) {
-                        cm = m;
-                        active = uniform_ld(&J.mdone[m], &shv) < 0 && uniform_ld(&J.mouter[m], &shv) > 0;
-                        if (active) {
-                            const int kinds[2] = {R_PQ, cur ? R_RZ1 : R_RZ0};
-                            double tot[2];
-                            member_totals<2>(J, m, kinds, tot, sh);
-                            alpha = (tot[0] != 0.0) ? tot[1] / tot[0] : 0.0;
+            const int cp = it & 1, np = cp ^ 1;
+            const float4* __restrict__ uwc = ir_uws(J, cp);
+            float4* __restrict__ uwn = ir_uws(J, np);
+            int cm = -1;
+            bool active = false;
+            float al = 0.0f, bt = 0.0f;
+            for (int t = tb0; t < tb1; t++) {
+                const int m = J.tile_mem[t];
+                if (m != cm) {
+                    cm = m;
+                    active = inner_member_on(J, m, it);
+                    if (active) {
+                        const int kinds[3] = {cp ? R_RZ1 : R_RZ0, cp ? R_WU1 : R_WU0, cp ? R_RR1 : R_RR0};
+                        double tot[3];
+                        member_totals<3>(J, m, kinds, tot, sh);
+                        const bool owner = (t == J.mem_t0[m] && tid == 0);
+                        if (it > 0 && checkpoint(J, it - 1, J.inner_maxiter) && tot[2] <= J.mem_atol2[nmem + m]) {
+                            active = false;
+                            if (owner) { J.mret[m] = it; J.minner[m] += it; }
+                        } else {
+                            double alpha, beta;
+                            if (it == 0) {
+                                beta = 0.0;
+                                alpha = (tot[1] != 0.0) ? tot[0] / tot[1] : 0.0;
+                            } else {
+                                const double ap = J.mem_ab[(size_t)np * nmem + m];
+                                const double gp = J.mem_ab[(size_t)(2 + np) * nmem + m];
+                                beta = (gp != 0.0) ? tot[0] / gp : 0.0;
+                                const double den = tot[1] - ((ap != 0.0) ? beta * tot[0] / ap : 0.0);
+                                alpha = (den != 0.0) ? tot[0] / den : 0.0;
+                            }
+                            if (owner) {
+                                J.mem_ab[(size_t)cp * nmem + m] = alpha;
+                                J.mem_ab[(size_t)(2 + cp) * nmem + m] = tot[0];
+                            }
+                            al = (float)alpha; bt = (float)beta;
                         }
                     }
-                    if (!active) continue;
-                    const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
-                    const float al = (float)alpha;
-                    double v[2] = {0.0, 0.0};
-                    for (int i = r0 + tid; i < r1; i += kThreads) {
-                        J.d32[i] += al * pn[i];
-                        const float ri = J.r32[i] - al * J.q32[i];
-                        const float zi = J.invD32[i] * ri;
-                        J.r32[i] = ri; J.z32[i] = zi;
-                        v[0] += (double)ri * (double)ri; v[1] += (double)ri * (double)zi;
-                    }
-                    const int kinds[2] = {srr, srz};
-                    put_partials<2>(J, t, kinds, v, sh);
                 }
+                if (!active) continue;
+                const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
+                double v[3] = {0.0, 0.0, 0.0};
+                for (int i = r0 + tid; i < r1; i += kThreads) {
+                    const float4 o = uwc[i];
+                    const float snew = o.y + bt * o.z;
+                    const float pnew = o.x + bt * pp[i];
+                    dd[i] += al * pnew;
+                    pp[i] = pnew;
+                    const float unew = u_next(o, al, bt);
+                    const float w = row_dot<SELL, float>(J, J.A32, i, [&](int c) { return u_next(uwc[c], al, bt); });
+                    uwn[i] = make_float4(unew, w, snew, 0.0f);
+                    const double dg = J.diag32[i], du = dg * unew;
+                    v[0] += du * unew; v[1] += dg * (double)w * unew; v[2] += du * du;
+                }
+                const int kinds[3] = {np ? R_RZ1 : R_RZ0, np ? R_WU1 : R_WU0, np ? R_RR1 : R_RR0};
+                put_partials<3>(J, t, kinds, v, sh);
             }
             GSYNC();
         }
-        total_inner += it;
-        // x += d for members that ran this sweep; restore the sweep markers
+        // x += d for the members of this sweep; the sweep's owner closes the member's count
+        // (members still on at the iteration cap count it in full)
         for (int t = tb0; t < tb1; t++) {
             const int m = J.tile_mem[t];
             if (uniform_ld(&J.mdone[m], &shv) >= 0) continue;
             const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
-            for (int i = r0 + tid; i < r1; i += kThreads) J.x[i] += (double)J.d32[i];
-        }
-        GSYNC();
-        for (int t = tb0; t < tb1; t++) {
-            const int m = J.tile_mem[t];
-            if (t == J.mem_t0[m] && tid == 0 && J.mouter[m] < 0) J.mouter[m] = -J.mouter[m];
+            for (int i = r0 + tid; i < r1; i += kThreads) J.x[i] += (double)dd[i];
+            if (t == J.mem_t0[m] && tid == 0 && J.mret[m] < 0) J.minner[m] += it;
         }
         GSYNC();
     }
     for (int t = tb0; t < tb1; t++) {
         const int m = J.tile_mem[t];
         if (t == J.mem_t0[m] && tid == 0 && ld_done(J, m) < 0) {
-            J.mdone[m] = total_inner;
+            J.mdone[m] = J.minner[m];
             atomicOr(J.err, ERR_JCG_NOT_CONVERGED);
         }
     }
@@ -469,10 +538,13 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
 
 struct JcgWork {
     int n = 0, nmem = 0, ntiles = 0, grid = 0, grid64 = 0, gridir = 0;
+    bool sell = false;               // kernels instantiated for the SELL-32 layout
     int32_t *tile_r0 = nullptr, *tile_r1 = nullptr, *tile_mem = nullptr, *mem_t0 = nullptr, *mem_t1 = nullptr;
     int32_t *blk64 = nullptr, *blkir = nullptr;
-    double *tile_part = nullptr, *mem_atol2 = nullptr;
-    int32_t *mdone = nullptr, *mouter = nullptr;
+    double *tile_part = nullptr, *mem_atol2 = nullptr, *mem_ab = nullptr;
+    // per-member control words in one array: mdone, mouter, minner, mret ([nmem] each), ndone
+    int32_t* mctl = nullptr;
+    int32_t *mdone = nullptr, *mouter = nullptr, *minner = nullptr, *mret = nullptr;
     unsigned* ndone = nullptr;
 };
 
@@ -496,7 +568,7 @@ static int coop_blocks(const void* fn, int nsm) {
     return nsm * per_sm;
 }
 
-cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std::vector<int>& rows) {
+cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std::vector<int>& rows, bool sell) {
     w = new JcgWork();
     const int nmem = (int)rows.size();
     std::vector<int32_t> tr0, tr1, tm, mt0(nmem), mt1(nmem);
@@ -516,8 +588,11 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    w->grid64 = std::max(1, std::min(T, coop_blocks((const void*)k_jcg64, nsm)));
-    w->gridir = std::max(1, std::min(T, coop_blocks((const void*)k_jcg_ir, nsm)));
+    const void* f64 = sell ? (const void*)k_jcg64<true> : (const void*)k_jcg64<false>;
+    const void* fir = sell ? (const void*)k_jcg_ir<true> : (const void*)k_jcg_ir<false>;
+    w->sell = sell;
+    w->grid64 = std::max(1, std::min(T, coop_blocks(f64, nsm)));
+    w->gridir = std::max(1, std::min(T, coop_blocks(fir, nsm)));
     std::vector<int32_t> b64, bir;
     block_ranges(T, w->grid64, b64);
     block_ranges(T, w->gridir, bir);
@@ -528,8 +603,11 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     A((void**)&w->blk64, 4 * b64.size()); A((void**)&w->blkir, 4 * bir.size());
     A((void**)&w->tile_part, 8 * (size_t)R_KINDS * T);
     A((void**)&w->mem_atol2, 16 * (size_t)nmem);
-    A((void**)&w->mdone, 4 * nmem); A((void**)&w->mouter, 4 * nmem); A((void**)&w->ndone, 8);
+    A((void**)&w->mem_ab, 32 * (size_t)nmem);
+    A((void**)&w->mctl, 4 * (4 * (size_t)nmem + 2));
     if (e != cudaSuccess) return e;
+    w->mdone = w->mctl; w->mouter = w->mctl + nmem; w->minner = w->mctl + 2 * nmem; w->mret = w->mctl + 3 * nmem;
+    w->ndone = (unsigned*)(w->mctl + 4 * nmem);
     cudaMemcpy(w->tile_r0, tr0.data(), 4 * T, cudaMemcpyHostToDevice);
     cudaMemcpy(w->tile_r1, tr1.data(), 4 * T, cudaMemcpyHostToDevice);
     cudaMemcpy(w->tile_mem, tm.data(), 4 * T, cudaMemcpyHostToDevice);
@@ -538,14 +616,14 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     cudaMemcpy(w->blk64, b64.data(), 4 * b64.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(w->blkir, bir.data(), 4 * bir.size(), cudaMemcpyHostToDevice);
     cudaMemset(w->tile_part, 0, 8 * (size_t)R_KINDS * T);
-    cudaMemset(w->mouter, 0, 4 * nmem);
+    cudaMemset(w->mctl, 0, 4 * (4 * (size_t)nmem + 2));
     return cudaGetLastError();
 }
 
 void jcg_work_free(JcgWork* w) {
     if (!w) return;
     void* ps[] = {w->tile_r0, w->tile_r1, w->tile_mem, w->mem_t0, w->mem_t1, w->blk64, w->blkir,
-                  w->tile_part, w->mem_atol2, w->mdone, w->mouter, w->ndone};
+                  w->tile_part, w->mem_atol2, w->mem_ab, w->mctl};
     for (void* p : ps) cudaFree(p);
     delete w;
 }
@@ -554,24 +632,25 @@ cudaError_t jcg_launch(const JcgArgs& a, JcgWork* w, cudaStream_t st, int nsm) {
     (void)nsm;
     JcgView J{};
     J.n = a.n; J.nmem = w->nmem; J.ntiles = w->ntiles;
-    J.indptr = a.indptr; J.indices = a.indices; J.A = a.A; J.A32 = a.A32; J.b = a.b; J.invD = a.invD;
+    J.indptr = a.indptr; J.sell = a.sell; J.indices = a.indices; J.A = a.A; J.A32 = a.A32; J.b = a.b; J.invD = a.invD;
     J.x = a.x; J.r = a.r; J.z = a.z; J.q = a.q; J.p0 = a.p0; J.p1 = a.p1;
-    J.r32 = a.r32; J.z32 = a.z32; J.q32 = a.q32; J.p032 = a.p032; J.p132 = a.p132; J.d32 = a.d32;
-    J.invD32 = a.invD32;
+    J.ir32 = a.ir32; J.diag32 = a.diag32;
     J.tile_r0 = w->tile_r0; J.tile_r1 = w->tile_r1; J.tile_mem = w->tile_mem;
     J.mem_t0 = w->mem_t0; J.mem_t1 = w->mem_t1;
     const bool ir = (a.precision == GS_FP32_IR);
     J.blk_t0 = ir ? w->blkir : w->blk64;
     J.tile_part = w->tile_part; J.mem_atol2 = w->mem_atol2;
-    J.mdone = w->mdone; J.mouter = w->mouter; J.ndone = w->ndone;
-    J.bar_count = a.bar_count; J.bar_gen = a.bar_gen; J.err = a.err;
+    J.mdone = w->mdone; J.mouter = w->mouter; J.minner = w->minner; J.mret = w->mret; J.ndone = w->ndone;
+    J.mem_ab = w->mem_ab;
+    J.bar = a.bar; J.err = a.err;
     J.rtol = a.rtol; J.maxiter = a.maxiter; J.check_every = a.check_every > 0 ? a.check_every : 1;
     J.inner_rtol = a.inner_rtol; J.inner_maxiter = a.inner_maxiter;
     cudaMemsetAsync(w->mdone, 0xFF, 4 * (size_t)w->nmem, st);
-    cudaMemsetAsync(w->ndone, 0, 8, st);
-    cudaMemsetAsync(w->mouter, 0, 4 * (size_t)w->nmem, st);
+    cudaMemsetAsync(w->mouter, 0, 4 * (3 * (size_t)w->nmem + 1), st);   // mouter, minner, mret, ndone
     void* args[] = {&J};
-    const void* fn = ir ? (const void*)k_jcg_ir : (const void*)k_jcg64;
+    if ((a.sell != nullptr) != w->sell) return cudaErrorInvalidValue;
+    const void* fn = ir ? (w->sell ? (const void*)k_jcg_ir<true> : (const void*)k_jcg_ir<false>)
+                        : (w->sell ? (const void*)k_jcg64<true> : (const void*)k_jcg64<false>);
     const int grid = ir ? w->gridir : w->grid64;
     return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, 0, st);
 }
@@ -610,7 +689,7 @@ constexpr size_t kNoAllocBytes = kNaOffCtl + kNaCtlBytes;                // abou
 static __device__ __align__(256) unsigned char gs_noalloc_scratch[kNoAllocBytes];
 
 // control words at kNaOffCtl: [0] mem_t0, [1] mem_t1, [2] mdone, [3] mouter, [4] ndone,
-// [5] bar_count, [6] bar_gen, [7] err
+// [5] grid barrier word, [6] unused, [7] err
 
 __global__ void k_noalloc_setup(unsigned char* base, int n, const int32_t* indptr, const int32_t* indices,
                                 const double* A, int ntiles, int grid) {
@@ -672,7 +751,7 @@ extern "C" gs_status gs_jcg_solve_csr_noalloc(int n, const int32_t* indptr, cons
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int ntiles = (n + kNoAllocTileRows - 1) / kNoAllocTileRows;
-    const int grid = std::max(1, std::min(ntiles, coop_blocks((const void*)k_jcg64, nsm)));
+    const int grid = std::max(1, std::min(ntiles, coop_blocks((const void*)k_jcg64<false>, nsm)));
     k_noalloc_setup<<<std::max(1, std::min(64, (n + 255) / 256)), 256, 0, st>>>(base, n, indptr, indices, data,
                                                                                ntiles, grid);
     int32_t* ctl = (int32_t*)(base + kNaOffCtl);
@@ -689,11 +768,11 @@ extern "C" gs_status gs_jcg_solve_csr_noalloc(int n, const int32_t* indptr, cons
     J.tile_mem = J.tile_r1 + kNoAllocMaxTiles;
     J.blk_t0 = (const int32_t*)(base + kNaOffBlk);
     J.mem_t0 = ctl + 0; J.mem_t1 = ctl + 1; J.mdone = ctl + 2; J.mouter = ctl + 3;
-    J.ndone = (unsigned*)(ctl + 4); J.bar_count = (unsigned*)(ctl + 5); J.bar_gen = (unsigned*)(ctl + 6);
+    J.ndone = (unsigned*)(ctl + 4); J.bar = (unsigned*)(ctl + 5);
     J.err = ctl + 7;
     J.rtol = rtol; J.maxiter = maxiter; J.check_every = check_every > 0 ? check_every : 1;
     void* args[] = {&J};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_jcg64, dim3(grid), dim3(kThreads), args, 0, st);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_jcg64<false>, dim3(grid), dim3(kThreads), args, 0, st);
     if (e != cudaSuccess) return GS_ERR_CUDA;
     int32_t h[8] = {0};
     e = cudaMemcpyAsync(h, ctl, sizeof(h), cudaMemcpyDeviceToHost, st);

@@ -16,8 +16,7 @@ struct gs_jcg {
     int32_t *indptr = nullptr, *indices = nullptr;
     double *A = nullptr, *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *q = nullptr, *p0 = nullptr,
            *p1 = nullptr, *invD = nullptr, *x0 = nullptr, *x1 = nullptr, *x2 = nullptr, *scratch = nullptr;
-    float *A32 = nullptr, *r32 = nullptr, *z32 = nullptr, *q32 = nullptr, *p032 = nullptr, *p132 = nullptr,
-          *d32 = nullptr, *invD32 = nullptr;
+    float *A32 = nullptr, *ir32 = nullptr, *diag32 = nullptr;
     unsigned *bar = nullptr;
     int32_t* err = nullptr;
     JcgWork* w = nullptr;
@@ -28,20 +27,22 @@ struct gs_jcg {
 namespace gs {
 
 __global__ void k_jcg_prep(int n, const int32_t* indptr, const int32_t* indices, const double* A, double* invD,
-                           float* invD32, double* x, const double* x0, const double* x1, const double* x2) {
-    // computeInvDiag (pcg_solver.py:933-938) and extrapolateGuess (:881-886)
+                           float* diag32, float* A32, double* x, const double* x0, const double* x1,
+                           const double* x2) {
+    // computeInvDiag (pcg_solver.py:933-938) and extrapolateGuess (:881-886); with A32 set, also
+    // the FP32 rows of D^-1 A and the FP32 diagonal of the refinement solve
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double dg = 0.0;
         for (int a = indptr[i]; a < indptr[i + 1]; a++)
             if (indices[a] == i) dg = A[a];
-        invD[i] = 1.0 / dg;
-        invD32[i] = (float)(1.0 / dg);
+        const double inv = 1.0 / dg;
+        invD[i] = inv;
+        if (A32) {
+            diag32[i] = (float)dg;
+            for (int a = indptr[i]; a < indptr[i + 1]; a++) A32[a] = (float)(A[a] * inv);
+        }
         x[i] = 3.0 * x0[i] - 3.0 * x1[i] + x2[i];
     }
-}
-
-__global__ void k_to_f32(int n, const double* a, float* b) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (float)a[i];
 }
 
 __global__ void k_roll(int n, const double* x, double* x0, double* x1, double* x2) {
@@ -95,10 +96,10 @@ gs_status gs_jcg_create(int n, int nnz, int precision, int device, gs_jcg** out)
 #define J(f, k) if (e == cudaSuccess) e = jalloc(s, s->f, k)
     J(indptr, n + 1); J(indices, nnz); J(A, nnz); J(A32, nnz);
     J(b, n); J(x, n); J(r, n); J(z, n); J(q, n); J(p0, n); J(p1, n); J(invD, n); J(x0, n); J(x1, n); J(x2, n);
-    J(scratch, 2); J(r32, n); J(z32, n); J(q32, n); J(p032, n); J(p132, n); J(d32, n); J(invD32, n);
+    J(scratch, 2); J(ir32, (size_t)kIrVectors * n); J(diag32, n);
     J(bar, 2); J(err, 1);
 #undef J
-    if (e == cudaSuccess) e = jcg_work_alloc(s->w, std::vector<int>{0}, std::vector<int>{n});
+    if (e == cudaSuccess) e = jcg_work_alloc(s->w, std::vector<int>{0}, std::vector<int>{n}, false);
     if (e != cudaSuccess) {
         gs_status st = (e == cudaErrorMemoryAllocation) ? GS_ERR_OOM : GS_ERR_CUDA;
         gs_jcg_destroy(s);
@@ -124,15 +125,16 @@ gs_status gs_jcg_solve_csr(gs_jcg* s, double rtol, int maxiter, int check_every,
     cudaSetDevice(s->dev);
     const int n = s->n;
     const int g = grid_for(n, 256, s->nsm * 8);
-    k_jcg_prep<<<g, 256, 0, s->st>>>(n, s->indptr, s->indices, s->A, s->invD, s->invD32, s->x, s->x0, s->x1, s->x2);
-    if (s->precision == GS_FP32_IR) k_to_f32<<<grid_for(s->nnz, 256, s->nsm * 8), 256, 0, s->st>>>(s->nnz, s->A, s->A32);
+    float* a32 = (s->precision == GS_FP32_IR) ? s->A32 : nullptr;
+    k_jcg_prep<<<g, 256, 0, s->st>>>(n, s->indptr, s->indices, s->A, s->invD, s->diag32, a32, s->x, s->x0, s->x1,
+                                     s->x2);
     JcgArgs a{};
     a.n = n; a.precision = s->precision;
     a.indptr = s->indptr; a.indices = s->indices; a.A = s->A; a.A32 = s->A32; a.b = s->b; a.invD = s->invD;
     a.x = s->x; a.r = s->r; a.z = s->z; a.q = s->q; a.p0 = s->p0; a.p1 = s->p1;
-    a.r32 = s->r32; a.z32 = s->z32; a.q32 = s->q32; a.p032 = s->p032; a.p132 = s->p132; a.d32 = s->d32;
-    a.invD32 = s->invD32;
-    a.bar_count = s->bar; a.bar_gen = s->bar + 1; a.err = s->err;
+    a.ir32 = s->ir32;
+    a.diag32 = s->diag32;
+    a.bar = s->bar; a.err = s->err;
     a.rtol = rtol; a.maxiter = maxiter; a.check_every = check_every < 1 ? 1 : check_every;
     a.inner_rtol = 1e-4; a.inner_maxiter = 400;
     cudaError_t e = jcg_launch(a, s->w, s->st, s->nsm);
@@ -144,7 +146,11 @@ gs_status gs_jcg_solve_csr(gs_jcg* s, double rtol, int maxiter, int check_every,
     int32_t flags = 0;
     cudaMemcpy(&flags, s->err, 4, cudaMemcpyDeviceToHost);
     if (iters) *iters = it[0];
-    if (flags & ERR_BARRIER_TIMEOUT) { s->msg = "device barrier timed out"; return GS_ERR_TIMEOUT; }
+    if (flags & ERR_BARRIER_TIMEOUT) {
+        cudaMemset(s->bar, 0, sizeof(unsigned));     // the barrier word is left mid-round
+        s->msg = "device barrier timed out";
+        return GS_ERR_TIMEOUT;
+    }
     return GS_OK;
 }
 

@@ -126,7 +126,7 @@ __global__ void k_assemble(Dev d, Phys P) {
     // setupCoefficientMatrixAndRHS (mdc:3182-3474) for one row per thread, then rollUpElevation
     // (mdc:3538) and setEssentialBC (mdc:4400-4446) on the same row, then the per-solve set-up
     // of PCGSolverMultiGPU.solve (b, invD, parabolic guess; pcg_solver.py:881-938).
-    const int NE = d.NE, NS = d.NS, NP = d.NP;
+    const int NE = d.NE, NP = d.NP;
     const double dt = P.dt, th = P.thetai;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NP; i += gridDim.x * blockDim.x) {
         const int q0 = d.nne_s[i], q1 = d.nne_s[i + 1];
@@ -198,17 +198,19 @@ __global__ void k_assemble(Dev d, Phys P) {
                 }
             }
         }
+        // FP64 row, and the row of D^-1 A in FP32 for the refinement solve
+        const double inv = 1.0 / diag;
         for (int p = 0; p < nn; p++) {
             const int at = d.nbr_slot[s0 + p];
             d.A[at] = vals[p];
-            d.A32[at] = (float)vals[p];
+            d.A32[at] = (float)(vals[p] * inv);
         }
         d.A[d.diag_slot[i]] = diag;
-        d.A32[d.diag_slot[i]] = (float)diag;
+        d.A32[d.diag_slot[i]] = 1.0f;
         d.qel[i] = qel;
         d.b[i] = qel;
-        d.invD[i] = 1.0 / diag;
-        d.invD32[i] = (float)(1.0 / diag);
+        d.invD[i] = inv;
+        d.diag32[i] = (float)diag;
         d.xs[i] = 3.0 * d.xh0[i] - 3.0 * d.xh1[i] + d.xh2[i];
     }
 }

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
         T.nsub[m] = 0;
     }
     if (gid == 0) *T.active = (unsigned)nmem;
-    if (!grid_sync(d.bar_count, d.bar_gen, d.err)) return;
+    if (!grid_sync(d.bar, d.err)) return;
     for (int sub = 0; sub < T.maxsub; sub++) {
         if (*((volatile unsigned*)T.active) == 0u) break;
         const int par = sub & 1, nxt = par ^ 1;
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
             d.maxDt[e] = md;
             atomicMin(&T.mindt[par * nmem + m], (unsigned long long)__double_as_longlong(md));
         }
-        if (!grid_sync(d.bar_count, d.bar_gen, d.err)) return;
+        if (!grid_sync(d.bar, d.err)) return;
         // horizontalAdvectionUpdate (meshdata.cu:6561-6609) with dtb = min(remaining, min maxDt)
         for (int e = gid; e < NE; e += G) {
             const int m = d.elem_member[e];
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
             }
             if (last) vertical_upwind(d, P, e, T.dt);
         }
-        if (!grid_sync(d.bar_count, d.bar_gen, d.err)) return;
+        if (!grid_sync(d.bar, d.err)) return;
     }
 }
 

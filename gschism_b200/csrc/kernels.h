@@ -12,13 +12,15 @@ struct VG;
 
 struct JcgArgs {
     int n, precision;
-    const int32_t *indptr, *indices;
+    const int32_t *indptr, *indices;     // CSR rows, or SELL-32 slices when sell is set
+    const int2* sell;
     const double* A;
-    const float* A32;
+    const float* A32;                    // D^-1 A in FP32
     const double *b, *invD;
     double *x, *r, *z, *q, *p0, *p1;
-    float *r32, *z32, *q32, *p032, *p132, *d32, *invD32;
-    unsigned *bar_count, *bar_gen;
+    float* ir32;                         // kIrVectors * n floats
+    const float* diag32;                 // matrix diagonal in FP32
+    unsigned* bar;
     int32_t* err;
     double rtol;
     int maxiter, check_every;
@@ -26,7 +28,7 @@ struct JcgArgs {
     int inner_maxiter;
 };
 struct JcgWork;
-cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std::vector<int>& rows);
+cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std::vector<int>& rows, bool sell);
 void jcg_work_free(JcgWork* w);
 cudaError_t jcg_launch(const JcgArgs& a, JcgWork* w, cudaStream_t st, int nsm);
 cudaError_t jcg_read_iters(JcgWork* w, std::vector<int>& iters, std::vector<int>& outer, cudaStream_t st);

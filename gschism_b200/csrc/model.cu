@@ -68,6 +68,8 @@ struct gs_ctx {
     int32_t* d_it = nullptr;
     std::string err;
     std::vector<int> last_iters, last_outer;
+    // batch CSR of the elevation matrix on the host (export) and each CSR entry's SELL position
+    std::vector<int32_t> h_indptr, h_indices, h_csr2sell;
     gs_status fail(gs_status s, const std::string& m) { err = m; return s; }
 };
 
@@ -387,7 +389,41 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
 
     // ------------------------------------------------------------------ device state
     Dev& d = c->d;
-    d.NP = NP; d.NE = NE; d.NS = NS; d.NNZ = (int)B.indices.size(); d.NB = (int)B.bn_node.size();
+    // SELL-32 layout of the batch matrix; assembly slots move to their SELL positions
+    std::vector<int2> sell;
+    std::vector<int32_t> sidx;
+    {
+        const int nsl = (NP + 31) / 32;
+        sell.resize(nsl);
+        c->h_csr2sell.assign(B.indices.size(), 0);
+        long long off = 0;
+        for (int s = 0; s < nsl; s++) {
+            int w = 0;
+            for (int i = 32 * s; i < std::min(NP, 32 * s + 32); i++) w = std::max(w, B.indptr[i + 1] - B.indptr[i]);
+            sell[s].x = (int)off; sell[s].y = w;
+            off += 32LL * w;
+            if (off > 0x7fffffffLL) return c->fail(GS_ERR_ARG, "elevation matrix too large for 32-bit offsets");
+        }
+        sidx.assign((size_t)off, 0);
+        for (int s = 0; s < nsl; s++)
+            for (int l = 0; l < 32; l++) {
+                const int i = 32 * s + l;
+                for (int k = 0; k < sell[s].y; k++) {
+                    const size_t pos = (size_t)sell[s].x + 32 * (size_t)k + l;
+                    if (i < NP && k < B.indptr[i + 1] - B.indptr[i]) {
+                        sidx[pos] = B.indices[B.indptr[i] + k];
+                        c->h_csr2sell[B.indptr[i] + k] = (int32_t)pos;
+                    } else {
+                        sidx[pos] = std::min(i, NP - 1);
+                    }
+                }
+            }
+        for (auto& v : B.nbr_slot) v = c->h_csr2sell[v];
+        for (auto& v : B.diag_slot) v = c->h_csr2sell[v];
+        c->h_indptr = B.indptr;
+        c->h_indices = B.indices;
+    }
+    d.NP = NP; d.NE = NE; d.NS = NS; d.NNZ = (int)sidx.size(); d.NB = (int)B.bn_node.size();
     d.nmem = (int)c->mem.size();
     cudaError_t e = cudaSuccess;
 #define UP(field, vec) if (e == cudaSuccess) e = dup(c, d.field, vec)
@@ -401,10 +437,10 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     UP(nbr_slot, B.nbr_slot); UP(diag_slot, B.diag_slot); UP(sb1, B.sb1); UP(sb2, B.sb2);
     UP(bn_node, B.bn_node); UP(bn_ietype, B.bn_ietype); UP(bn_nbfr, B.bn_nbfr);
     UP(bn_emo, B.bn_emo); UP(bn_efa, B.bn_efa); UP(bn_amig, B.bn_amig); UP(bn_ff, B.bn_ff); UP(bn_face, B.bn_face);
-    UP(indptr, B.indptr); UP(indices, B.indices); AL(A, d.NNZ); AL(A32, d.NNZ);
+    UP(sell, sell); UP(indices, sidx); AL(A, d.NNZ); AL(A32, d.NNZ);
     AL(b, NP); AL(xs, NP); AL(r, NP); AL(zz, NP); AL(p0, NP); AL(p1, NP); AL(q, NP); AL(invD, NP);
     AL(xh0, NP); AL(xh1, NP); AL(xh2, NP);
-    AL(r32, NP); AL(z32, NP); AL(p032, NP); AL(p132, NP); AL(q32, NP); AL(d32, NP); AL(invD32, NP);
+    AL(ir32, (size_t)kIrVectors * NP); AL(diag32, NP);
     UP(sn, B.sn); UP(se, B.se); UP(len, B.len); UP(snx, B.snx); UP(sny, B.sny); UP(scx, B.scx); UP(scy, B.scy);
     UP(cori, B.cori); AL(kbs, NS); AL(sdry, NS); UP(sbt, B.sbt);
     AL(zc, (size_t)nvrt * NS); AL(Qh, (size_t)nvrt * NS); AL(su2, (size_t)nvrt * NS); AL(btu, (size_t)nvrt * NS);
@@ -416,14 +452,14 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     UP(etr, B.etr); AL(prev, (size_t)ntr * nvrt * NE); AL(maxDt, NE); AL(ghat, NE);
     UP(mem_np0, B.mem_np0); UP(mem_ne0, B.mem_ne0); UP(elem_member, B.elem_member);
     AL(mem_rem, 2 * (size_t)d.nmem); AL(mem_dtb, d.nmem); AL(mem_mindt, 2 * (size_t)d.nmem + 1); AL(mem_nsub, d.nmem);
-    AL(bar_count, 1); AL(bar_gen, 1); AL(err, 1); AL(counters, 4);
+    AL(bar, 1); AL(err, 1); AL(counters, 4);
 #undef UP
 #undef AL
     if (e != cudaSuccess) return c->fail(e == cudaErrorMemoryAllocation ? GS_ERR_OOM : GS_ERR_CUDA, cudaGetErrorString(e));
     {
         std::vector<int> row0, rows;
         for (auto& m : c->mem) { row0.push_back(m.np0); rows.push_back(m.np); }
-        e = jcg_work_alloc(c->jw, row0, rows);
+        e = jcg_work_alloc(c->jw, row0, rows, true);
         if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
     }
     // constants
@@ -474,10 +510,10 @@ static gs_status run_phase(gs_ctx* c, int phase, int arg) {
         JcgArgs a{};
         Dev& d = c->d;
         a.n = d.NP; a.precision = c->cfg.precision;
-        a.indptr = d.indptr; a.indices = d.indices; a.A = d.A; a.A32 = d.A32; a.b = d.b; a.invD = d.invD;
+        a.indptr = nullptr; a.sell = d.sell; a.indices = d.indices; a.A = d.A; a.A32 = d.A32; a.b = d.b; a.invD = d.invD;
         a.x = d.xs; a.r = d.r; a.z = d.zz; a.q = d.q; a.p0 = d.p0; a.p1 = d.p1;
-        a.r32 = d.r32; a.z32 = d.z32; a.q32 = d.q32; a.p032 = d.p032; a.p132 = d.p132; a.d32 = d.d32; a.invD32 = d.invD32;
-        a.bar_count = d.bar_count; a.bar_gen = d.bar_gen; a.err = d.err;
+        a.ir32 = d.ir32; a.diag32 = d.diag32;
+        a.bar = d.bar; a.err = d.err;
         a.rtol = c->cfg.rtol; a.maxiter = c->cfg.maxiter; a.check_every = c->cfg.check_every;
         a.inner_rtol = c->cfg.ir_inner_rtol; a.inner_maxiter = c->cfg.ir_inner_maxiter;
         cudaError_t e = jcg_launch(a, c->jw, st, nsm);
@@ -506,7 +542,10 @@ static gs_status check_err(gs_ctx* c) {
     cudaError_t e = cudaMemcpyAsync(&flags, c->d.err, 4, cudaMemcpyDeviceToHost, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
     if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
-    if (flags & ERR_BARRIER_TIMEOUT) return c->fail(GS_ERR_TIMEOUT, "a bounded device barrier timed out");
+    if (flags & ERR_BARRIER_TIMEOUT) {
+        cudaMemsetAsync(c->d.bar, 0, sizeof(unsigned), c->st);   // the barrier word is left mid-round
+        return c->fail(GS_ERR_TIMEOUT, "a bounded device barrier timed out");
+    }
     if (flags & ERR_DEGREE) return c->fail(GS_ERR_BAD_MESH, "node degree above the supported maximum");
     return GS_OK;
 }
@@ -649,13 +688,12 @@ void member_csr(gs_ctx* c, MemberHost& m, std::vector<int32_t>& indptr, std::vec
     const Connectivity& C = m.con;
     indptr.assign(m.np + 1, 0);
     indices.clear(); src.clear();
-    std::vector<int32_t> hind(m.nnz), hptr(m.np + 1);
-    cudaMemcpy(hind.data(), c->d.indices + m.nnz0, 4 * (size_t)m.nnz, cudaMemcpyDeviceToHost);
-    cudaMemcpy(hptr.data(), c->d.indptr + m.np0, 4 * (size_t)(m.np + 1), cudaMemcpyDeviceToHost);
+    const std::vector<int32_t>& hptr = c->h_indptr;
+    const std::vector<int32_t>& hind = c->h_indices;
     for (int o = 0; o < m.np; o++) {
-        const int i = m.qn[o];
+        const int i = m.np0 + m.qn[o];
         std::vector<std::pair<int, int>> row;
-        for (int a = hptr[i]; a < hptr[i + 1]; a++) row.push_back({m.pn[hind[a - m.nnz0 + 0] - m.np0], a});
+        for (int a = hptr[i]; a < hptr[i + 1]; a++) row.push_back({m.pn[hind[a] - m.np0], c->h_csr2sell[a]});
         std::sort(row.begin(), row.end());
         for (auto& pr : row) { indices.push_back(pr.first); src.push_back(pr.second); }
         indptr[o + 1] = (int)indices.size();
@@ -683,10 +721,10 @@ extern "C" gs_status gs_state_get(gs_ctx* c, int member, int field, void* host, 
             std::memcpy(host, ix.data(), bytes);
         } else {
             if (bytes != 8 * src.size()) return c->fail(GS_ERR_STATE, "size");
-            std::vector<double> all(m.nnz);
-            cudaMemcpy(all.data(), c->d.A + m.nnz0, 8 * (size_t)m.nnz, cudaMemcpyDeviceToHost);
+            std::vector<double> all(c->d.NNZ);
+            cudaMemcpy(all.data(), c->d.A, 8 * (size_t)c->d.NNZ, cudaMemcpyDeviceToHost);
             double* out = (double*)host;
-            for (size_t a = 0; a < src.size(); a++) out[a] = all[src[a] - m.nnz0];
+            for (size_t a = 0; a < src.size(); a++) out[a] = all[src[a]];
         }
         return GS_OK;
     }
