@@ -548,16 +548,29 @@ struct JcgWork {
     unsigned* ndone = nullptr;
 };
 
-// tile rows of a member: a function of the member's own size only (batch independence)
+// Tile rows of a member: a function of the member's own size only (batch independence).  A
+// large member is cut into about kMemberTiles tiles, i.e. one per block of a 4-blocks-per-SM grid
+// on a 148-SM part, so its rows spread evenly over the SMs; tiles never go below 256 rows.
+constexpr int kMemberTiles = 592;
 static int tile_rows_for(int rows) {
-    int t = 256;
-    while (t < 4096 && (rows + t - 1) / t > 512) t *= 2;
-    return t;
+    const long long per = ((long long)rows + kMemberTiles - 1) / kMemberTiles;
+    return (int)std::max(256LL, (per + 31) / 32 * 32);
 }
 
-static void block_ranges(int ntiles, int grid, std::vector<int32_t>& bt) {
-    bt.resize(grid + 1);
-    for (int b = 0; b <= grid; b++) bt[b] = (int32_t)((long long)ntiles * b / grid);
+// Contiguous tile ranges per block with about the same number of rows in each.
+static void block_ranges(const std::vector<int32_t>& tr0, const std::vector<int32_t>& tr1, int grid,
+                         std::vector<int32_t>& bt) {
+    const int T = (int)tr0.size();
+    std::vector<long long> cum(T + 1, 0);
+    for (int t = 0; t < T; t++) cum[t + 1] = cum[t] + (tr1[t] - tr0[t]);
+    bt.assign(grid + 1, T);
+    bt[0] = 0;
+    int t = 0;
+    for (int b = 1; b < grid; b++) {
+        const long long target = cum[T] * b / grid;
+        while (t < T && cum[t] + (tr1[t] - tr0[t]) / 2 < target) t++;
+        bt[b] = std::max(bt[b - 1], t);
+    }
 }
 
 static int coop_blocks(const void* fn, int nsm) {
@@ -594,8 +607,8 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     w->grid64 = std::max(1, std::min(T, coop_blocks(f64, nsm)));
     w->gridir = std::max(1, std::min(T, coop_blocks(fir, nsm)));
     std::vector<int32_t> b64, bir;
-    block_ranges(T, w->grid64, b64);
-    block_ranges(T, w->gridir, bir);
+    block_ranges(tr0, tr1, w->grid64, b64);
+    block_ranges(tr0, tr1, w->gridir, bir);
     cudaError_t e = cudaSuccess;
     auto A = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes ? bytes : 8); };
     A((void**)&w->tile_r0, 4 * T); A((void**)&w->tile_r1, 4 * T); A((void**)&w->tile_mem, 4 * T);

@@ -1,0 +1,42 @@
+"""Run a synthetic case for a few steps and print the per-step solver statistics.
+
+    python -m gschism_b200.run_case --case basin --n 1000 --levels 6 --steps 2 --precision fp32_ir
+
+Used to drive profiler captures of one phase on a chosen size: the elevation solve depends on
+the horizontal mesh only, so `--levels` can shrink the device state without changing it.
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+from . import cases
+from .model import Model
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--case", choices=["basin", "channel"], default="basin")
+    ap.add_argument("--n", type=int, default=1000, help="basin lattice side (n x n nodes)")
+    ap.add_argument("--levels", type=int, default=30, help="vertical levels (basin)")
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--precision", choices=["fp64", "fp32_ir"], default="fp32_ir")
+    ap.add_argument("--inner-rtol", type=float, default=1e-4)
+    a = ap.parse_args(argv)
+    t0 = time.time()
+    if a.case == "basin":
+        c = cases.basin(n=a.n, nvrt=a.levels, nz=max(2, min(10, a.levels // 3)))
+    else:
+        c = cases.channel()
+    m = Model([c], precision=a.precision, ir_inner_rtol=a.inner_rtol)
+    print(f"case {a.case}: {m.sizes[0]['np']} nodes, {c.vgrid.nvrt} levels, set-up {time.time() - t0:.1f} s",
+          flush=True)
+    for s in range(a.steps):
+        m.step(1)
+        m.sync()
+        print("step", s, m.stats(), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
