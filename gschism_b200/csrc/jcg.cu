@@ -48,6 +48,10 @@ struct JcgView {
     int32_t* minner;               // [nmem] inner iterations so far (IR)
     int32_t* mret;                 // [nmem] inner iteration at which the sweep's solve finished, -1 before
     double* mem_ab;                // [4][nmem] alpha (parity 0, 1) and gamma (parity 0, 1) of the inner solve
+    double* mpub;                  // [nmem][2] published (alpha, beta) of the member's current inner iteration
+    int32_t* mgen;                 // [nmem] inner iteration whose scalars are published (kRetired: finished)
+    unsigned* mcnt;                // [nmem] block arrivals of the inner solve
+    const int32_t* mnblk;          // [nmem] blocks of the refinement grid that hold tiles of the member
     unsigned* ndone;
     unsigned* bar;
     int32_t* err;
@@ -364,18 +368,93 @@ __device__ __forceinline__ float u_next(float4 q, float al, float bt) { return q
 
 __device__ __forceinline__ int ld_i32(const int32_t* p) { return *((const volatile int32_t*)p); }
 
-// a member takes part in inner iteration it unless it retired before it (mret is written once
-// per sweep, with the iteration at which the member met the inner tolerance, during that very
-// iteration; both values a block may read then lead to the same decision)
-__device__ __forceinline__ bool inner_member_on(const JcgView& J, int m, int it) {
-    if (ld_i32(&J.mdone[m]) >= 0 || ld_i32(&J.mouter[m]) <= 0) return false;
-    const int r = ld_i32(&J.mret[m]);
-    return r < 0 || r >= it;
+// ---- member-level synchronisation of the inner solve.  Rows of a member only couple to rows of
+// the same member, so the inner iterations need no grid-wide barrier: after its tiles of member m
+// a block adds one to mcnt[m]; the block whose arrival completes the member's count (mnblk[m]
+// blocks hold its tiles) sums the member's tile partials in tile order, takes the convergence
+// decision, computes the next (alpha, beta) and publishes them with mgen[m] = next iteration (or
+// kRetired).  Blocks wait only for the members they hold.  Every wait is bounded.
+constexpr int kRetired = 0x7fffffff;
+
+__device__ __forceinline__ int ld_acquire_i32(const int32_t* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_i32(int32_t* p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Wait until member m has published inner iteration it.  pub receives (alpha, beta, state) with
+// state 1 = on, 0 = finished, -1 = failed wait (the caller leaves the kernel).
+__device__ __forceinline__ void member_wait(const JcgView& J, int m, int it, double* pub) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long spins = 0;
+        int g;
+        bool ok = true;
+        while ((g = ld_acquire_i32(&J.mgen[m])) < it) {
+            if (++spins > 4096) __nanosleep(128);
+            if (spins > (1ll << 24)) { atomicOr(J.err, ERR_BARRIER_TIMEOUT); ok = false; break; }
+            if ((spins & 255) == 0 && (*((volatile int32_t*)J.err) & ERR_BARRIER_TIMEOUT)) { ok = false; break; }
+        }
+        __threadfence();
+        if (!ok) {
+            pub[2] = -1.0;
+        } else if (g == kRetired) {
+            pub[2] = 0.0;
+        } else {
+            pub[0] = __ldcg(&J.mpub[2 * m]);
+            pub[1] = __ldcg(&J.mpub[2 * m + 1]);
+            pub[2] = 1.0;
+        }
+    }
+    __syncthreads();
+}
+
+// This block's tiles of member m are done for inner iteration it (their partials of iteration
+// it + 1 are in parity slot np).  The member's last arriver publishes iteration it + 1.
+__device__ __forceinline__ void member_arrive(const JcgView& J, int m, int it, int np, double* sh, int* shv) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned old = atomicAdd(&J.mcnt[m], 1u);
+        const bool last = ((old + 1u) % (unsigned)J.mnblk[m]) == 0u;
+        if (last) __threadfence();
+        *shv = last ? 1 : 0;
+    }
+    __syncthreads();
+    if (!*shv) return;
+    const int kinds[3] = {np ? R_RZ1 : R_RZ0, np ? R_WU1 : R_WU0, np ? R_RR1 : R_RR0};
+    double tot[3];
+    member_totals<3>(J, m, kinds, tot, sh);
+    if (threadIdx.x != 0) return;
+    const int nmem = J.nmem, nit = it + 1;
+    if (checkpoint(J, it, J.inner_maxiter) && tot[2] <= J.mem_atol2[nmem + m]) {
+        J.mret[m] = nit;
+        J.minner[m] += nit;
+        __threadfence();
+        st_release_i32(&J.mgen[m], kRetired);
+        return;
+    }
+    const int cp = np ^ 1;
+    const double ap = J.mem_ab[(size_t)cp * nmem + m];
+    const double gp = J.mem_ab[(size_t)(2 + cp) * nmem + m];
+    const double beta = (gp != 0.0) ? tot[0] / gp : 0.0;
+    const double den = tot[1] - ((ap != 0.0) ? beta * tot[0] / ap : 0.0);
+    const double alpha = (den != 0.0) ? tot[0] / den : 0.0;
+    J.mem_ab[(size_t)np * nmem + m] = alpha;
+    J.mem_ab[(size_t)(2 + np) * nmem + m] = tot[0];
+    J.mpub[2 * m] = alpha;
+    J.mpub[2 * m + 1] = beta;
+    __threadfence();
+    st_release_i32(&J.mgen[m], nit);
 }
 
 template <bool SELL>
 __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
     __shared__ double sh[4 * 32];
+    __shared__ double pub[3];
     __shared__ int shv;
     const int tid = threadIdx.x;
     const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
@@ -434,6 +513,8 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
                     J.mem_atol2[nmem + m] = J.inner_rtol * J.inner_rtol * tot[0];
                     J.mouter[m] = outer + 1;
                     J.mret[m] = -1;
+                    J.mgen[m] = 0;
+                    J.mcnt[m] = 0u;
                 }
                 const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
                 double v[3] = {0.0, 0.0, 0.0};
@@ -450,51 +531,43 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
         }
         GSYNC();
         if (*((volatile unsigned*)J.ndone) >= (unsigned)nmem) break;
-        int it = 0;
-        for (; it < J.inner_maxiter; it++) {
-            bool any = false;
-            for (int m = 0; m < nmem && !any; m++) any = inner_member_on(J, m, it);
-            if (!any) break;
+        // inner iterations: iteration 0's scalars come from the O2 totals (every block forms them);
+        // later ones are published per member by its last arriver
+        for (int it = 0; it < J.inner_maxiter; it++) {
             const int cp = it & 1, np = cp ^ 1;
             const float4* __restrict__ uwc = ir_uws(J, cp);
             float4* __restrict__ uwn = ir_uws(J, np);
+            bool any = false;
             int cm = -1;
-            bool active = false;
+            bool on = false;
             float al = 0.0f, bt = 0.0f;
             for (int t = tb0; t < tb1; t++) {
                 const int m = J.tile_mem[t];
                 if (m != cm) {
+                    if (cm >= 0 && on) member_arrive(J, cm, it, np, sh, &shv);
                     cm = m;
-                    active = inner_member_on(J, m, it);
-                    if (active) {
-                        const int kinds[3] = {cp ? R_RZ1 : R_RZ0, cp ? R_WU1 : R_WU0, cp ? R_RR1 : R_RR0};
-                        double tot[3];
-                        member_totals<3>(J, m, kinds, tot, sh);
-                        const bool owner = (t == J.mem_t0[m] && tid == 0);
-                        if (it > 0 && checkpoint(J, it - 1, J.inner_maxiter) && tot[2] <= J.mem_atol2[nmem + m]) {
-                            active = false;
-                            if (owner) { J.mret[m] = it; J.minner[m] += it; }
-                        } else {
-                            double alpha, beta;
-                            if (it == 0) {
-                                beta = 0.0;
-                                alpha = (tot[1] != 0.0) ? tot[0] / tot[1] : 0.0;
-                            } else {
-                                const double ap = J.mem_ab[(size_t)np * nmem + m];
-                                const double gp = J.mem_ab[(size_t)(2 + np) * nmem + m];
-                                beta = (gp != 0.0) ? tot[0] / gp : 0.0;
-                                const double den = tot[1] - ((ap != 0.0) ? beta * tot[0] / ap : 0.0);
-                                alpha = (den != 0.0) ? tot[0] / den : 0.0;
+                    if (it == 0) {
+                        on = uniform_ld(&J.mdone[m], &shv) < 0;
+                        if (on) {
+                            const int kinds[2] = {R_RZ0, R_WU0};
+                            double tot[2];
+                            member_totals<2>(J, m, kinds, tot, sh);
+                            const double alpha = (tot[1] != 0.0) ? tot[0] / tot[1] : 0.0;
+                            if (t == J.mem_t0[m] && tid == 0) {
+                                J.mem_ab[m] = alpha;
+                                J.mem_ab[(size_t)2 * nmem + m] = tot[0];
                             }
-                            if (owner) {
-                                J.mem_ab[(size_t)cp * nmem + m] = alpha;
-                                J.mem_ab[(size_t)(2 + cp) * nmem + m] = tot[0];
-                            }
-                            al = (float)alpha; bt = (float)beta;
+                            al = (float)alpha; bt = 0.0f;
                         }
+                    } else {
+                        member_wait(J, m, it, pub);
+                        if (pub[2] < -0.5) return;
+                        on = pub[2] > 0.5;
+                        al = (float)pub[0]; bt = (float)pub[1];
                     }
                 }
-                if (!active) continue;
+                if (!on) continue;
+                any = true;
                 const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
                 double v[3] = {0.0, 0.0, 0.0};
                 for (int i = r0 + tid; i < r1; i += kThreads) {
@@ -512,7 +585,8 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
                 const int kinds[3] = {np ? R_RZ1 : R_RZ0, np ? R_WU1 : R_WU0, np ? R_RR1 : R_RR0};
                 put_partials<3>(J, t, kinds, v, sh);
             }
-            GSYNC();
+            if (cm >= 0 && on) member_arrive(J, cm, it, np, sh, &shv);
+            if (!any) break;
         }
         // x += d for the members of this sweep; the sweep's owner closes the member's count
         // (members still on at the iteration cap count it in full)
@@ -521,7 +595,7 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
             if (uniform_ld(&J.mdone[m], &shv) >= 0) continue;
             const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
             for (int i = r0 + tid; i < r1; i += kThreads) J.x[i] += (double)dd[i];
-            if (t == J.mem_t0[m] && tid == 0 && J.mret[m] < 0) J.minner[m] += it;
+            if (t == J.mem_t0[m] && tid == 0 && J.mret[m] < 0) J.minner[m] += J.inner_maxiter;
         }
         GSYNC();
     }
@@ -542,9 +616,11 @@ struct JcgWork {
     int32_t *tile_r0 = nullptr, *tile_r1 = nullptr, *tile_mem = nullptr, *mem_t0 = nullptr, *mem_t1 = nullptr;
     int32_t *blk64 = nullptr, *blkir = nullptr;
     double *tile_part = nullptr, *mem_atol2 = nullptr, *mem_ab = nullptr;
-    // per-member control words in one array: mdone, mouter, minner, mret ([nmem] each), ndone
+    // per-member control words in one array: mdone, mouter, minner, mret, mgen, mcnt ([nmem] each), ndone
     int32_t* mctl = nullptr;
-    int32_t *mdone = nullptr, *mouter = nullptr, *minner = nullptr, *mret = nullptr;
+    int32_t *mdone = nullptr, *mouter = nullptr, *minner = nullptr, *mret = nullptr, *mgen = nullptr;
+    unsigned* mcnt = nullptr;
+    int32_t* mnblk = nullptr;
     unsigned* ndone = nullptr;
 };
 
@@ -616,11 +692,23 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     A((void**)&w->blk64, 4 * b64.size()); A((void**)&w->blkir, 4 * bir.size());
     A((void**)&w->tile_part, 8 * (size_t)R_KINDS * T);
     A((void**)&w->mem_atol2, 16 * (size_t)nmem);
-    A((void**)&w->mem_ab, 32 * (size_t)nmem);
-    A((void**)&w->mctl, 4 * (4 * (size_t)nmem + 2));
+    A((void**)&w->mem_ab, 48 * (size_t)nmem);
+    A((void**)&w->mctl, 4 * (6 * (size_t)nmem + 2));
+    A((void**)&w->mnblk, 4 * (size_t)nmem);
     if (e != cudaSuccess) return e;
     w->mdone = w->mctl; w->mouter = w->mctl + nmem; w->minner = w->mctl + 2 * nmem; w->mret = w->mctl + 3 * nmem;
-    w->ndone = (unsigned*)(w->mctl + 4 * nmem);
+    w->mgen = w->mctl + 4 * nmem; w->mcnt = (unsigned*)(w->mctl + 5 * nmem);
+    w->ndone = (unsigned*)(w->mctl + 6 * nmem);
+    {
+        // blocks of the refinement grid holding tiles of each member
+        std::vector<int32_t> nb(nmem, 0);
+        for (int b = 0; b < w->gridir; b++) {
+            int last = -1;
+            for (int t = bir[b]; t < bir[b + 1]; t++)
+                if (tm[t] != last) { last = tm[t]; nb[last]++; }
+        }
+        cudaMemcpy(w->mnblk, nb.data(), 4 * (size_t)nmem, cudaMemcpyHostToDevice);
+    }
     cudaMemcpy(w->tile_r0, tr0.data(), 4 * T, cudaMemcpyHostToDevice);
     cudaMemcpy(w->tile_r1, tr1.data(), 4 * T, cudaMemcpyHostToDevice);
     cudaMemcpy(w->tile_mem, tm.data(), 4 * T, cudaMemcpyHostToDevice);
@@ -629,14 +717,14 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     cudaMemcpy(w->blk64, b64.data(), 4 * b64.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(w->blkir, bir.data(), 4 * bir.size(), cudaMemcpyHostToDevice);
     cudaMemset(w->tile_part, 0, 8 * (size_t)R_KINDS * T);
-    cudaMemset(w->mctl, 0, 4 * (4 * (size_t)nmem + 2));
+    cudaMemset(w->mctl, 0, 4 * (6 * (size_t)nmem + 2));
     return cudaGetLastError();
 }
 
 void jcg_work_free(JcgWork* w) {
     if (!w) return;
     void* ps[] = {w->tile_r0, w->tile_r1, w->tile_mem, w->mem_t0, w->mem_t1, w->blk64, w->blkir,
-                  w->tile_part, w->mem_atol2, w->mem_ab, w->mctl};
+                  w->tile_part, w->mem_atol2, w->mem_ab, w->mctl, w->mnblk};
     for (void* p : ps) cudaFree(p);
     delete w;
 }
@@ -654,12 +742,13 @@ cudaError_t jcg_launch(const JcgArgs& a, JcgWork* w, cudaStream_t st, int nsm) {
     J.blk_t0 = ir ? w->blkir : w->blk64;
     J.tile_part = w->tile_part; J.mem_atol2 = w->mem_atol2;
     J.mdone = w->mdone; J.mouter = w->mouter; J.minner = w->minner; J.mret = w->mret; J.ndone = w->ndone;
-    J.mem_ab = w->mem_ab;
+    J.mem_ab = w->mem_ab; J.mpub = w->mem_ab + 4 * (size_t)w->nmem;
+    J.mgen = w->mgen; J.mcnt = w->mcnt; J.mnblk = w->mnblk;
     J.bar = a.bar; J.err = a.err;
     J.rtol = a.rtol; J.maxiter = a.maxiter; J.check_every = a.check_every > 0 ? a.check_every : 1;
     J.inner_rtol = a.inner_rtol; J.inner_maxiter = a.inner_maxiter;
     cudaMemsetAsync(w->mdone, 0xFF, 4 * (size_t)w->nmem, st);
-    cudaMemsetAsync(w->mouter, 0, 4 * (3 * (size_t)w->nmem + 1), st);   // mouter, minner, mret, ndone
+    cudaMemsetAsync(w->mouter, 0, 4 * (5 * (size_t)w->nmem + 1), st);   // mouter .. mcnt, ndone
     void* args[] = {&J};
     if ((a.sell != nullptr) != w->sell) return cudaErrorInvalidValue;
     const void* fn = ir ? (w->sell ? (const void*)k_jcg_ir<true> : (const void*)k_jcg_ir<false>)
