@@ -626,11 +626,14 @@ struct JcgWork {
 
 // Tile rows of a member: a function of the member's own size only (batch independence).  A
 // large member is cut into about kMemberTiles tiles, i.e. one per block of a 4-blocks-per-SM grid
-// on a 148-SM part, so its rows spread evenly over the SMs; tiles never go below 256 rows.
+// on a 148-SM part, so its rows spread evenly over the SMs.  Tiles never go below kMinTileRows
+// (four rows per thread): every tile ends in a block-wide reduction, and smaller tiles leave too
+// little independent work between those reductions.
 constexpr int kMemberTiles = 592;
+constexpr int kMinTileRows = 1024;
 static int tile_rows_for(int rows) {
     const long long per = ((long long)rows + kMemberTiles - 1) / kMemberTiles;
-    return (int)std::max(256LL, (per + 31) / 32 * 32);
+    return (int)std::max((long long)kMinTileRows, (per + 31) / 32 * 32);
 }
 
 // Contiguous tile ranges per block with about the same number of rows in each.
