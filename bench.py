@@ -13,6 +13,9 @@ e2e      = the same loop through the C ABI with host buffers: every step uploads
            stress field from host memory (gs_set_tau) and reads the elevation back (gs_state_get).
 roofline = the JCG persistent kernel (dominant), algorithmic bytes per launch / launch time.
 The plain FP64 single-instance form is measured on the same GPU and reported under "fp64".
+ensemble = the batched form: 64 members on meshes of uneven size (20k-500k nodes, 20 levels,
+           1 tracer, per-member tide and wind), all members in one launch per phase, FP32+IR and
+           FP64, against the plain FP64 single-instance form run member by member.
 Multi-GPU (torchrun): every rank steps its own replica of the mesh (no data exchange exists in
 the step); value = all ranks' node-level-steps / the max over ranks of the device time.
 """
@@ -37,12 +40,13 @@ METRIC = "node-level-steps/s"
 def _args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1000, help="lattice side (n x n nodes)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble comparison")
     return ap.parse_args()
 
 
@@ -78,7 +82,7 @@ class Clocks:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -116,6 +120,12 @@ class Clocks:
         out["reasons"] = sorted(reasons)
         out["samples"] = len(sm)
         return out
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per inner iteration of k_jcg_ir on
+# the 1M-node basin, from the ncu capture summarised in profiles/k_jcg_ir_basin1M.md (launch
+# bytes / inner iterations of that launch); scaled here by the timed launches' inner iterations.
+JCG_DRAM_BYTES_PER_INNER_ITER = 31.6e6
 
 
 def _jcg_bytes_per_iter(N, nnz, mode):
@@ -214,6 +224,8 @@ def run_ours(a):
         dist.destroy_process_group()
     if rank != 0:
         return
+    # the batched-ensemble comparison is a one-GPU measurement (rank 0 of a one-rank run)
+    ens = run_ensemble(a, stream, local) if (ws == 1 and not a.no_ensemble) else None
     r = res["fp32_ir"]
     # roofline of the dominant kernel (JCG): algorithmic bytes / average launch time
     nnz = r["nnz"]
@@ -232,7 +244,9 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (state ~10 GB per replica)"},
         "e2e": r["e2e"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "kernel": "k_jcg_ir",
+                     "frac": achieved / peak,
+                     "traffic": (None if JCG_DRAM_BYTES_PER_INNER_ITER is None
+                                 else JCG_DRAM_BYTES_PER_INNER_ITER * it_in), "kernel": "k_jcg_ir",
                      "peak_kind": peak_kind, "iters_per_launch": it_in, "bytes_per_launch": bytes_launch},
         "clocks": r["clocks"],
         "gpu_launches": a.steps * 18,
@@ -242,12 +256,65 @@ def run_ours(a):
         f = res["fp64"]
         line["fp64"] = {"value": f["value"], "ms_per_step": f["ms_per_step"], "jcg_iters": f["jcg_iters_last"],
                         "jcg_ms_avg": statistics.mean(f["jcg_ms"])}
+    if ens is not None:
+        line["ensemble"] = ens
     if not a.no_cpu:
         line["cpu_baseline"] = cpu_sample(a)
     print(json.dumps(line))
 
 
-def cpu_sample(a, steps=2, n=200):
+def run_ensemble(a, stream, local):
+    """64-member ensemble: batched FP32+IR and FP64 (one launch per phase for all members) and
+    the plain FP64 single-instance form (one member at a time), same steps, device time."""
+    import torch
+    from gschism_b200 import cases
+    from gschism_b200.model import Model
+    ens = cases.ensemble(n_members=64)
+    nodes = sum(c.n_nodes for c in ens)
+    nvrt = ens[0].vgrid.nvrt
+    steps, warm = min(a.steps, 5), max(3, min(a.warmup, 3))
+
+    def timed(m):
+        m.set_stream(stream.cuda_stream)
+        for _ in range(warm):
+            m.step(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            m.step(1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    out = {"workload": f"64 members, {nodes} nodes in total (20k-500k each, log-uniform), {nvrt} levels, "
+                       f"1 tracer, per-member tide 0.3-2 m and wind stress 0-0.3 N/m2, dt=120 s",
+           "nodes": nodes, "levels": nvrt, "steps": steps, "warmup": warm}
+    eta = {}
+    for prec in ("fp32_ir", "fp64"):
+        m = Model(ens, precision=prec, device=local)
+        ms = timed(m)
+        its = [m.stats(i)["jcg_iters"] for i in range(len(ens))]
+        eta[prec] = [m.get(i, "ETA2").copy() for i in range(len(ens))]
+        out[f"{prec}_batched"] = {"value": nodes * nvrt / (ms / 1e3), "ms_per_step": ms,
+                                  "jcg_iters_min": min(its), "jcg_iters_max": max(its)}
+        m.close()
+        del m
+        torch.cuda.empty_cache()
+    out["max_eta_diff_fp32_ir_vs_fp64_m"] = max(float(np.max(np.abs(x - y))) for x, y in zip(eta["fp32_ir"], eta["fp64"]))
+    tot = 0.0
+    for c in ens:
+        m = Model([c], precision="fp64", device=local)
+        tot += timed(m)
+        m.close()
+        del m
+    out["fp64_single_instance"] = {"value": nodes * nvrt / (tot / 1e3), "ms_per_step": tot,
+                                   "note": "members stepped one at a time, sum of their device times"}
+    out["speedup_fp32_ir_batched_vs_fp64_single"] = tot / out["fp32_ir_batched"]["ms_per_step"]
+    return out
+
+
+def cpu_sample(a, steps=6, n=500):
     """The CPU restatement (oracle) on a bounded sample of the same workload: a n x n basin with
     the same levels, tracers and physics, all host threads, `steps` steps."""
     from gschism_b200 import cases
@@ -268,7 +335,7 @@ def run_reference(a):
         return
     from gschism_b200 import cases
     from oracle.step_api import OracleModel
-    n = 200
+    n = 500
     case = cases.basin(seed=2, n=n, nvrt=30, nz=10, ntr=2, length=500e3 * n / 1000)
     o = OracleModel(case)
     for _ in range(min(a.warmup, 1)):
