@@ -47,7 +47,9 @@ struct JcgView {
     int32_t* mouter;               // [nmem] refinement sweeps (IR)
     int32_t* minner;               // [nmem] inner iterations so far (IR)
     int32_t* mret;                 // [nmem] inner iteration at which the sweep's solve finished, -1 before
-    double* mem_ab;                // [4][nmem] alpha (parity 0, 1) and gamma (parity 0, 1) of the inner solve
+    double* mem_ab;                // [9][nmem] inner solve: alpha (parity 0, 1), gamma (parity 0, 1),
+                                   // [4..6) published (alpha, beta) pairs, [6] alpha, [7] gamma and
+                                   // [8] recursive r.r of the previous sweep's last iteration
     double* mpub;                  // [nmem][2] published (alpha, beta) of the member's current inner iteration
     int32_t* mgen;                 // [nmem] inner iteration whose scalars are published (kRetired: finished)
     unsigned* mcnt;                // [nmem] block arrivals of the inner solve
@@ -430,14 +432,22 @@ __device__ __forceinline__ void member_arrive(const JcgView& J, int m, int it, i
     member_totals<3>(J, m, kinds, tot, sh);
     if (threadIdx.x != 0) return;
     const int nmem = J.nmem, nit = it + 1;
-    if (checkpoint(J, it, J.inner_maxiter) && tot[2] <= J.mem_atol2[nmem + m]) {
+    const int cp = np ^ 1;
+    const bool done = checkpoint(J, it, J.inner_maxiter) && tot[2] <= J.mem_atol2[nmem + m];
+    if (done || nit == J.inner_maxiter) {
+        // the sweep ends after iteration it: keep its (alpha, gamma) and recursive r.r for the
+        // next sweep
+        J.mem_ab[(size_t)6 * nmem + m] = J.mem_ab[(size_t)cp * nmem + m];
+        J.mem_ab[(size_t)7 * nmem + m] = J.mem_ab[(size_t)(2 + cp) * nmem + m];
+        J.mem_ab[(size_t)8 * nmem + m] = tot[2];
+    }
+    if (done) {
         J.mret[m] = nit;
         J.minner[m] += nit;
         __threadfence();
         st_release_i32(&J.mgen[m], kRetired);
         return;
     }
-    const int cp = np ^ 1;
     const double ap = J.mem_ab[(size_t)cp * nmem + m];
     const double gp = J.mem_ab[(size_t)(2 + cp) * nmem + m];
     const double beta = (gp != 0.0) ? tot[0] / gp : 0.0;
@@ -466,7 +476,10 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
     phase_atol(J, sh);
     GSYNC();
     for (int outer = 0; outer < 64; outer++) {
-        // O1: FP64 residual r = b - A x; u_0 = D^-1 r in FP32; s~, p, d = 0; outer r.r partials
+        // O1: FP64 residual r = b - A x; u_0 = D^-1 r in FP32 replaces the inner solve's recursive
+        // residual, d = 0; the search direction p and s~ = D^-1 A p carry over from the previous
+        // sweep (residual replacement: the inner CG continues instead of restarting; the first
+        // sweep starts from p = s~ = 0); outer r.r partials
         {
             float4* uw0 = ir_uws(J, 0);
             for (int t = tb0; t < tb1; t++) {
@@ -478,12 +491,21 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
                         for (int i = r0 + tid; i < r1; i += kThreads) J.x[i] = 0.0;
                     continue;
                 }
+                // parity holding the previous sweep's last s~ (its final inner iteration index)
+                int last = 0;
+                if (outer > 0) {
+                    const int rt = uniform_ld(&J.mret[m], &shv);
+                    last = (rt >= 0 ? rt : J.inner_maxiter) & 1;
+                }
+                const float4* uwl = ir_uws(J, last);
                 double v[1] = {0.0};
                 for (int i = r0 + tid; i < r1; i += kThreads) {
                     const double s = row_dot<SELL, double>(J, J.A, i, [&](int c) { return J.x[c]; });
                     const double ri = J.b[i] - s;
-                    uw0[i] = make_float4((float)(J.invD[i] * ri), 0.0f, 0.0f, 0.0f);
-                    pp[i] = 0.0f; dd[i] = 0.0f;
+                    const float sprev = (outer > 0) ? uwl[i].z : 0.0f;
+                    uw0[i] = make_float4((float)(J.invD[i] * ri), 0.0f, sprev, 0.0f);
+                    if (outer == 0) pp[i] = 0.0f;
+                    dd[i] = 0.0f;
                     v[0] += ri * ri;
                 }
                 const int kinds[1] = {R_OUT};
@@ -549,15 +571,29 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
                     if (it == 0) {
                         on = uniform_ld(&J.mdone[m], &shv) < 0;
                         if (on) {
-                            const int kinds[2] = {R_RZ0, R_WU0};
-                            double tot[2];
-                            member_totals<2>(J, m, kinds, tot, sh);
-                            const double alpha = (tot[1] != 0.0) ? tot[0] / tot[1] : 0.0;
+                            const int kinds[3] = {R_RZ0, R_WU0, R_RR0};
+                            double tot[3];
+                            member_totals<3>(J, m, kinds, tot, sh);
+                            // first sweep: beta = 0.  Later sweeps continue the recurrence from the
+                            // previous sweep's last (alpha, gamma) -- residual replacement every
+                            // inner_rtol reduction, which keeps the FP32 recursion accurate when
+                            // inner_rtol >= 1e-2 -- unless the replaced residual is more than 4x the
+                            // recursive one it replaces (r.r more than 16x).  Tighter inner
+                            // tolerances, or such a jump, restart the recurrence (beta = 0): plain
+                            // restarted refinement.
+                            const bool reliable = J.inner_rtol >= 1e-2;
+                            const double ac = (outer > 0) ? J.mem_ab[(size_t)6 * nmem + m] : 0.0;
+                            const double gc = (outer > 0) ? J.mem_ab[(size_t)7 * nmem + m] : 0.0;
+                            const double rc = (outer > 0) ? J.mem_ab[(size_t)8 * nmem + m] : 0.0;
+                            const bool cont = reliable && gc != 0.0 && ac != 0.0 && tot[2] <= 16.0 * rc;
+                            const double beta = cont ? tot[0] / gc : 0.0;
+                            const double den = tot[1] - ((beta != 0.0) ? beta * tot[0] / ac : 0.0);
+                            const double alpha = (den != 0.0) ? tot[0] / den : 0.0;
                             if (t == J.mem_t0[m] && tid == 0) {
                                 J.mem_ab[m] = alpha;
                                 J.mem_ab[(size_t)2 * nmem + m] = tot[0];
                             }
-                            al = (float)alpha; bt = 0.0f;
+                            al = (float)alpha; bt = (float)beta;
                         }
                     } else {
                         member_wait(J, m, it, pub);
@@ -695,7 +731,7 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     A((void**)&w->blk64, 4 * b64.size()); A((void**)&w->blkir, 4 * bir.size());
     A((void**)&w->tile_part, 8 * (size_t)R_KINDS * T);
     A((void**)&w->mem_atol2, 16 * (size_t)nmem);
-    A((void**)&w->mem_ab, 48 * (size_t)nmem);
+    A((void**)&w->mem_ab, 72 * (size_t)nmem);
     A((void**)&w->mctl, 4 * (6 * (size_t)nmem + 2));
     A((void**)&w->mnblk, 4 * (size_t)nmem);
     if (e != cudaSuccess) return e;

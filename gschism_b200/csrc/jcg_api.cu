@@ -136,7 +136,7 @@ gs_status gs_jcg_solve_csr(gs_jcg* s, double rtol, int maxiter, int check_every,
     a.diag32 = s->diag32;
     a.bar = s->bar; a.err = s->err;
     a.rtol = rtol; a.maxiter = maxiter; a.check_every = check_every < 1 ? 1 : check_every;
-    a.inner_rtol = 1e-4; a.inner_maxiter = 400;
+    a.inner_rtol = 0.1; a.inner_maxiter = 400;
     cudaError_t e = jcg_launch(a, s->w, s->st, s->nsm);
     if (e != cudaSuccess) { s->msg = cudaGetErrorString(e); return GS_ERR_CUDA; }
     k_roll<<<g, 256, 0, s->st>>>(n, s->x, s->x0, s->x1, s->x2);

@@ -129,7 +129,7 @@ gs_status gs_ctx_create(const gs_config* cfg, gs_ctx** out) {
     if (c->cfg.check_every < 1) c->cfg.check_every = 1;
     if (c->cfg.maxiter < 1) c->cfg.maxiter = 1;
     if (c->cfg.ir_inner_maxiter < 1) c->cfg.ir_inner_maxiter = 200;
-    if (!(c->cfg.ir_inner_rtol > 0.0)) c->cfg.ir_inner_rtol = 1e-4;
+    if (!(c->cfg.ir_inner_rtol > 0.0)) c->cfg.ir_inner_rtol = 0.1;
     *out = c;
     return GS_OK;
 }

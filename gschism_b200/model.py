@@ -47,7 +47,7 @@ def _flat(segs):
 class Model:
     def __init__(self, cases: Sequence[Case], precision: str = "fp64", device: int = 0,
                  rtol: float | None = None, maxiter: int | None = None, check_every: int | None = None,
-                 ir_inner_rtol: float = 1e-4, ir_inner_maxiter: int = 400):
+                 ir_inner_rtol: float = 0.1, ir_inner_maxiter: int = 400):
         self.lib = L.load()
         self.cases: List[Case] = list(cases)
         c0 = self.cases[0]

@@ -65,8 +65,12 @@ typedef struct {
     int ihhat;
     double rtol; int maxiter, check_every; /* JCG: pcg_solver.py:1075 solve(rtol, maxiter, checkEvery) */
     int precision;                         /* GS_FP64 or GS_FP32_IR */
-    double ir_inner_rtol;                  /* FP32 inner solve: stop at this relative residual */
-    int ir_inner_maxiter;
+    double ir_inner_rtol;                  /* FP32 inner solve: each refinement sweep reduces the
+                                              residual by this factor (<= 0: 0.1).  At >= 1e-2 the
+                                              sweeps replace the inner CG's residual with the FP64
+                                              one and continue its recurrence; tighter values
+                                              restart the inner CG every sweep. */
+    int ir_inner_maxiter;                  /* iteration cap of one sweep (< 1: 200) */
     int device;                            /* CUDA device ordinal */
 } gs_config;
 
