@@ -25,7 +25,8 @@ PHASE = dict(BEGIN=0, BTRACK=1, PREPARE=2, ASSEMBLE=3, SOLVE=4, UPDATE_ELEV=5, M
 EXPORTS = ["gs_grid_build", "gs_ctx_create", "gs_member_add", "gs_ctx_finalize", "gs_ctx_destroy",
            "gs_last_error", "gs_sync", "gs_set_stream", "gs_step", "gs_phase", "gs_state_get", "gs_state_put", "gs_set_tau",
            "gs_get_stats", "gs_member_sizes", "gs_jcg_create", "gs_jcg_buffers", "gs_jcg_solve_csr",
-           "gs_jcg_check", "gs_jcg_destroy", "gs_jcg_last_error", "gs_jcg_solve_csr_noalloc"]
+           "gs_jcg_check", "gs_jcg_destroy", "gs_jcg_last_error", "gs_jcg_solve_csr_noalloc",
+           "gs_set_vortex", "gs_footprint_bytes"]
 
 
 class GsConfig(ctypes.Structure):
@@ -44,6 +45,11 @@ class GsMemberDesc(ctypes.Structure):
                 ("x", PD), ("y", PD), ("depth", PD), ("drag", PD), ("tau", PD), ("tr_init", PD),
                 ("elnode", PI), ("open_start", PI), ("open_nodes", PI), ("land_start", PI), ("land_nodes", PI),
                 ("iettype", PI), ("amig", PD), ("ff", PD), ("face", PD), ("emo", PD), ("efa", PD)]
+
+
+class GsVortex(ctypes.Structure):
+    _fields_ = [("x0", c_double), ("y0", c_double), ("heading", c_double), ("speed", c_double),
+                ("vmax", c_double), ("rmax", c_double), ("holland_b", c_double), ("rho_air", c_double)]
 
 
 class GsStats(ctypes.Structure):
@@ -97,9 +103,12 @@ def load(build_if_missing: bool = False):
     L.gs_jcg_last_error.restype = ctypes.c_char_p
     L.gs_jcg_solve_csr_noalloc.argtypes = [I, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double, I, I,
                                            c_void_p, ctypes.POINTER(c_int)]
+    L.gs_set_vortex.argtypes = [c_void_p, I, ctypes.POINTER(GsVortex)]
+    L.gs_footprint_bytes.argtypes = [I, I, I, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64]
     for name in EXPORTS:
-        if name not in ("gs_last_error", "gs_jcg_last_error"):
+        if name not in ("gs_last_error", "gs_jcg_last_error", "gs_footprint_bytes"):
             getattr(L, name).restype = c_int
+    L.gs_footprint_bytes.restype = c_size_t
     _lib = L
     return L
 

@@ -334,6 +334,30 @@ def ensemble(n_members: int = 64, seed: int = 3, nmin: int = 20_000, nmax: int =
     return out
 
 
+def storm(seed: int, nmin: int = 10_000, nmax: int = 2_000_000, nvrt: int = 20, dt: float = 150.0,
+          hours: float = 48.0, shuffle: bool = True):
+    """A storm-surge forecast request: a basin mesh with a node count log-uniform in [nmin, nmax]
+    (500 m spacing), 20 levels, 1 tracer, tidal forcing on the west side (0.3-1.0 m), and a radial
+    vortex on a straight track crossing the domain: seeded heading, speed 3-8 m/s, maximum wind
+    20-60 m/s at a radius of 20-60 km (Holland B 1.2-1.8).  Returns (case, vortex, nsteps) with
+    nsteps covering `hours` at `dt`."""
+    rng = np.random.default_rng(seed)
+    target = math.exp(rng.uniform(math.log(nmin), math.log(nmax)))
+    side = max(8, int(round(math.sqrt(target))))
+    length = 500.0 * side
+    amp = rng.uniform(0.3, 1.0)
+    c = basin(seed=int(rng.integers(1, 2**31 - 1)), n=side, nvrt=nvrt, nz=max(2, nvrt // 3), ntr=1,
+              length=length, amp=amp, shuffle=shuffle, dt=dt)
+    c.name = f"storm{seed}"
+    heading = rng.uniform(0.0, 2.0 * math.pi)
+    # start 3/4 of the domain size behind the centre, so the track crosses the domain
+    cx, cy = 0.5 * length, 0.5 * length
+    vortex = dict(x0=cx - 0.75 * length * math.cos(heading), y0=cy - 0.75 * length * math.sin(heading),
+                  heading=heading, speed=rng.uniform(3.0, 8.0), vmax=rng.uniform(20.0, 60.0),
+                  rmax=rng.uniform(20e3, 60e3), holland_b=rng.uniform(1.2, 1.8), rho_air=1.15)
+    return c, vortex, int(round(hours * 3600.0 / dt))
+
+
 # ----------------------------------------------------------------------------------------------
 # SCHISM file formats
 # ----------------------------------------------------------------------------------------------

@@ -22,6 +22,7 @@ constexpr int kMaxTracers = 8;
 constexpr int kMaxLevels = 64;
 constexpr int kMaxBfr = 8;
 constexpr int kMaxDeg = 24;        // max node degree supported by the per-row assembly
+constexpr int kVortexParams = 9;  // x0, y0, heading, speed, vmax, rmax, B, rho_air, enabled
 constexpr int kIrVectors = 10;     // FP32 vectors of the refinement solve: (u, w, s, -) x 2, p, d
 
 // Device error bits (gs_stats.error_flags)
@@ -92,6 +93,7 @@ struct Dev {
     double2 *ghat;
     // members
     int32_t *mem_np0, *mem_ne0;    // entity offsets [nmem+1]
+    double *vort;                  // [nmem][kVortexParams] storm parameters (gs_vortex + enabled flag)
     int32_t *elem_member;          // [NE]
     double *mem_rem, *mem_dtb;     // transport sub-cycling per member
     unsigned long long *mem_mindt; // positive doubles ordered as unsigned

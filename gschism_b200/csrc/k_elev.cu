@@ -225,7 +225,41 @@ __global__ void k_update_elev(Dev d, VG vg) {
     }
 }
 
-void launch_elev_prepare(const Dev& d, const Phys& P, double time, double ramp, cudaStream_t st, int nsm) {
+// Storm forcing: kinematic surface stress of a radial vortex on a straight track (gs_vortex in the
+// C ABI) for the nodes of members that have one; other members keep their stress.
+__global__ void k_vortex_tau(Dev d, double time, double ramp, double rho0) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.NP; i += gridDim.x * blockDim.x) {
+        int lo = 0, hi = d.nmem;                       // member of node i: mem_np0[lo] <= i < mem_np0[lo+1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (d.mem_np0[mid] <= i) lo = mid; else hi = mid;
+        }
+        const double* v = d.vort + (size_t)kVortexParams * lo;
+        if (v[8] == 0.0) continue;
+        const double x0 = v[0], y0 = v[1], hd = v[2], sp = v[3], vmax = v[4], rmax = v[5], B = v[6], rho_air = v[7];
+        const double ch = cos(hd), sh = sin(hd);
+        const double cx = x0 + sp * time * ch, cy = y0 + sp * time * sh;
+        const double dx = d.x[i] - cx, dy = d.y[i] - cy;
+        const double r = sqrt(dx * dx + dy * dy);
+        double W = 0.0, tx = 0.0, ty = 0.0;
+        if (r > 1.0) {
+            const double q = pow(rmax / r, B);
+            W = vmax * sqrt(q * exp(1.0 - q));
+            tx = -dy / r; ty = dx / r;
+        }
+        const double f = W / vmax;
+        const double wx = W * tx + f * sp * ch, wy = W * ty + f * sp * sh;
+        const double ws = sqrt(wx * wx + wy * wy);
+        double cd = 1e-3 * (0.75 + 0.067 * ws);
+        if (cd > 3e-3) cd = 3e-3;
+        const double k = ramp * rho_air / rho0 * cd * ws;
+        d.tau[2 * (size_t)i] = k * wx;
+        d.tau[2 * (size_t)i + 1] = k * wy;
+    }
+}
+
+void launch_elev_prepare(const Dev& d, const Phys& P, double time, double ramp, bool vortex, cudaStream_t st, int nsm) {
+    if (vortex) k_vortex_tau<<<grid_for(d.NP, 256, nsm * 8), 256, 0, st>>>(d, time, ramp, P.rho0);
     if (d.NB > 0) k_elev_bc<<<grid_for(d.NB, 128, nsm * 4), 128, 0, st>>>(d, time, ramp);
     k_side_prep<<<grid_for(d.NS, 256, nsm * 16), 256, 0, st>>>(d, P);
     k_ghat<<<grid_for(d.NE, 256, nsm * 16), 256, 0, st>>>(d, P);

@@ -70,6 +70,9 @@ struct gs_ctx {
     std::vector<int> last_iters, last_outer;
     // batch CSR of the elevation matrix on the host (export) and each CSR entry's SELL position
     std::vector<int32_t> h_indptr, h_indices, h_csr2sell;
+    // storm parameters per member ([nmem][kVortexParams]) and how many members have one
+    std::vector<double> h_vort;
+    int nvortex = 0;
     gs_status fail(gs_status s, const std::string& m) { err = m; return s; }
 };
 
@@ -451,6 +454,8 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     AL(ez, (size_t)nvrt * NE); AL(ew, (size_t)nvrt * NE); AL(Qv, (size_t)nvrt * NE);
     UP(etr, B.etr); AL(prev, (size_t)ntr * nvrt * NE); AL(maxDt, NE); AL(ghat, NE);
     UP(mem_np0, B.mem_np0); UP(mem_ne0, B.mem_ne0); UP(elem_member, B.elem_member);
+    c->h_vort.assign((size_t)kVortexParams * c->mem.size(), 0.0);
+    UP(vort, c->h_vort);
     AL(mem_rem, 2 * (size_t)d.nmem); AL(mem_dtb, d.nmem); AL(mem_mindt, 2 * (size_t)d.nmem + 1); AL(mem_nsub, d.nmem);
     AL(bar, 1); AL(err, 1); AL(counters, 4);
 #undef UP
@@ -502,7 +507,7 @@ static gs_status run_phase(gs_ctx* c, int phase, int arg) {
     switch (phase) {
     case GS_PHASE_BEGIN: c->it = arg; break;
     case GS_PHASE_BTRACK: launch_btrack(c->d, c->P, c->vg, st, nsm); break;
-    case GS_PHASE_PREPARE: launch_elev_prepare(c->d, c->P, time, ramp_of(c, time), st, nsm); break;
+    case GS_PHASE_PREPARE: launch_elev_prepare(c->d, c->P, time, ramp_of(c, time), c->nvortex > 0, st, nsm); break;
     case GS_PHASE_ASSEMBLE:
         launch_assemble(c->d, c->P, st, nsm);
         break;
@@ -645,6 +650,7 @@ bool field_info(gs_ctx* c, int f, FieldInfo& fi) {
     case GS_F_ETA1: fi.ptr = d.eta1; return true;
     case GS_F_ETA2: fi.ptr = d.eta2; return true;
     case GS_F_QEL: fi.ptr = d.qel; return true;
+    case GS_F_NODE_TAU: fi.comp = 2; fi.ptr = d.tau; return true;
     case GS_F_ELBC: fi.ptr = d.elbc; return true;
     case GS_F_JCG_X: fi.ptr = d.xh0; return true;
     case GS_F_JCG_X1: fi.ptr = d.xh1; return true;
@@ -794,9 +800,48 @@ extern "C" gs_status gs_state_put(gs_ctx* c, int member, int field, const void* 
 extern "C" gs_status gs_set_tau(gs_ctx* c, int member, const double* tau_host) {
     if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size() || !tau_host) return GS_ERR_ARG;
     MemberHost& m = c->mem[member];
+    m.tau.assign(tau_host, tau_host + 2 * (size_t)m.np);        // restored when a storm is switched off
     std::vector<double> buf(2 * (size_t)m.np);
     for (int i = 0; i < m.np; i++) { buf[2 * i] = tau_host[2 * m.pn[i]]; buf[2 * i + 1] = tau_host[2 * m.pn[i] + 1]; }
     cudaError_t e = cudaMemcpyAsync(c->d.tau + 2 * (size_t)m.np0, buf.data(), buf.size() * 8, cudaMemcpyHostToDevice, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
     return e == cudaSuccess ? GS_OK : c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+extern "C" gs_status gs_set_vortex(gs_ctx* c, int member, const gs_vortex* v) {
+    if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size()) return GS_ERR_ARG;
+    if (v && !(v->vmax > 0.0 && v->rmax > 0.0 && v->holland_b > 0.0 && v->rho_air > 0.0))
+        return c->fail(GS_ERR_ARG, "vortex: vmax, rmax, holland_b and rho_air must be positive");
+    double* p = c->h_vort.data() + (size_t)kVortexParams * member;
+    const bool was = p[8] != 0.0;
+    if (v) {
+        const double q[kVortexParams] = {v->x0, v->y0, v->heading, v->speed, v->vmax, v->rmax, v->holland_b, v->rho_air, 1.0};
+        for (int k = 0; k < kVortexParams; k++) p[k] = q[k];
+    } else {
+        for (int k = 0; k < kVortexParams; k++) p[k] = 0.0;
+    }
+    c->nvortex += (v ? 1 : 0) - (was ? 1 : 0);
+    cudaError_t e = cudaMemcpyAsync(c->d.vort + (size_t)kVortexParams * member, p, sizeof(double) * kVortexParams,
+                                    cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    if (!v && was) return gs_set_tau(c, member, c->mem[member].tau.data());   // back to the member's own stress
+    return GS_OK;
+}
+
+// Upper bound of the device bytes gs_ctx_finalize allocates for members of these total sizes
+// (the allocation list of gs_ctx_finalize and jcg_work_alloc; boundary nodes counted as all nodes,
+// SELL padding as a quarter of the entries, plus allocation granularity).
+extern "C" size_t gs_footprint_bytes(int nvrt, int ntr, int nmem, int64_t np, int64_t ne, int64_t ns, int64_t nnz) {
+    if (nvrt < 1 || ntr < 0 || nmem < 1 || np < 0 || ne < 0 || ns < 0 || nnz < 0) return 0;
+    const double L = nvrt, T = ntr;
+    const double sell = (double)nnz * 1.25 + 32.0 * kMaxDeg;
+    double b = 0.0;
+    b += (double)np * (91.0 + L * (8 + 8 + 16 + 8 * T) + 20.0 + 88.0 + 4.0 * kIrVectors + 4.0 + 332.0);
+    b += (double)ne * (24.0 + 88.0 + 24.0 + 4.0 + L * (24.0 + 16.0 * T));
+    b += (double)ns * (16.0 + 70.0 + 72.0 + 16.0 + L * 52.0);
+    b += sell * 16.0 + (double)np / 32.0 * 8.0;
+    b += ((double)np / 1024.0 + nmem) * 84.0 + (double)nmem * (16.0 + 72.0 + 40.0 + 8.0 * kVortexParams + 64.0);
+    b += 256.0 * 1024 * 1024;                   // allocation granularity of ~120 allocations
+    return (size_t)b;
 }

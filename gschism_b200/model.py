@@ -19,13 +19,25 @@ import numpy as np
 from . import _lib as L
 from .cases import Case
 
-FIELDS = dict(ETA1=0, ETA2=1, NODE_Z=2, NODE_U2=3, NODE_W2=4, NODE_TR=5, NODE_KB=6, NODE_DRY=7, QEL=8,
+FIELDS = dict(ETA1=0, ETA2=1, NODE_Z=2, NODE_U2=3, NODE_W2=4, NODE_TR=5, NODE_KB=6, NODE_DRY=7, QEL=8, NODE_TAU=9,
               SIDE_U2=10, SIDE_BTU=11, SIDE_ZC=12, SIDE_KB=13, SIDE_DRY=14, SIDE_U=15, SIDE_HHAT=16,
               SIDE_CHI=17, SIDE_QH=18, SIDE_BTELEM=19, SIDE_GRADETA1=20, SIDE_GRADETA2=21,
               ELEM_Z=30, ELEM_W=31, ELEM_QV=32, ELEM_TR=33, ELEM_KB=34, ELEM_DRY=35, ELEM_GHAT=36,
               CSR_DATA=40, CSR_INDPTR=41, CSR_INDICES=42, JCG_X=43, ELBC=44, JCG_X1=45, JCG_X2=46)
 INT_FIELDS = {"NODE_KB", "NODE_DRY", "SIDE_KB", "SIDE_DRY", "SIDE_BTELEM", "ELEM_KB", "ELEM_DRY",
               "CSR_INDPTR", "CSR_INDICES"}
+
+
+def footprint_bytes(cases: Sequence[Case]) -> int:
+    """Upper bound of the device memory a context holding these members allocates
+    (gs_footprint_bytes).  Side and matrix counts follow from the triangulation: a simply
+    connected triangulated domain has np + ne - 1 sides and np + 2 ns matrix entries."""
+    lib = L.load()
+    c0 = cases[0]
+    npn = sum(c.n_nodes for c in cases)
+    ne = sum(c.n_elems for c in cases)
+    ns = sum(c.n_nodes + c.n_elems - 1 for c in cases)
+    return int(lib.gs_footprint_bytes(c0.vgrid.nvrt, c0.ntracers, len(cases), npn, ne, ns, npn + 2 * ns))
 
 
 def _pd(a):
@@ -155,6 +167,8 @@ class Model:
             return (n[table[name][0]],)
         if name in ("SIDE_U", "SIDE_GRADETA1", "SIDE_GRADETA2"):
             return (n["S"], 2)
+        if name == "NODE_TAU":
+            return (n["N"], 2)
         if name == "ELEM_GHAT":
             return (n["E"], 2)
         if name in ("NODE_Z", "NODE_W2"):
@@ -189,6 +203,15 @@ class Model:
             raise ValueError(f"{name}: shape {a.shape} != {self.shape(member, name)}")
         L.check(self.lib.gs_state_put(self.h, member, FIELDS[name], a.ctypes.data_as(ctypes.c_void_p), a.nbytes),
                 self.h, f"gs_state_put {name}")
+
+    def set_vortex(self, member: int, vortex) -> None:
+        """Storm forcing of a member (gs_set_vortex): a mapping with x0, y0, heading, speed, vmax,
+        rmax, holland_b, rho_air, or None to switch it off."""
+        if vortex is None:
+            L.check(self.lib.gs_set_vortex(self.h, member, None), self.h, "gs_set_vortex")
+            return
+        v = L.GsVortex(**{k: float(vortex[k]) for k, _ in L.GsVortex._fields_})
+        L.check(self.lib.gs_set_vortex(self.h, member, ctypes.byref(v)), self.h, "gs_set_vortex")
 
     def set_tau(self, member: int, tau) -> None:
         a = np.ascontiguousarray(tau, dtype=np.float64)

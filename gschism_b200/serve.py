@@ -1,0 +1,279 @@
+"""Forecast serving on one GPU: continuous batching of storm-surge requests.
+
+    python -m gschism_b200.serve --requests 16 --rate 2 --hours 48 [--seed 1] [--budget-gb 150]
+
+Requests (a mesh with its forcing and a horizon in steps) arrive over time.  The server keeps a
+FIFO queue and, at every scheduling turn, admits the longest prefix of the queue whose device
+memory (`footprint_bytes`, an upper bound of what the context allocates) fits in the memory left
+by the running work: the admitted requests become one cohort, a batch context holding them all
+as members.  New cohorts are built on a worker thread (host preprocessing and upload) while the
+running cohorts keep stepping, and join the stepping as soon as they are built.  Every turn
+advances each running cohort by a few steps; a cohort whose requests reach their horizon hands
+back its results, releases its memory and leaves.  So requests that arrive while others run are
+admitted as memory frees up and their steps interleave with the running ones, turn by turn.
+
+All cohorts step on one CUDA stream: the step's persistent kernels (elevation solve, transport)
+wait on each other's blocks and are never run concurrently with another such kernel.  Only the
+regular kernels of a cohort being built overlap them.  A member's results do not depend on the
+batch it runs in (per-member reductions in a fixed order), so each forecast is the same alone
+and in the mix.
+
+Reported: time-to-forecast per request (arrival to results on the host), its p50/p99, and the
+node-level-steps/s of the whole run.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import dataclasses
+import json
+import math
+import time
+from typing import Any, Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    case: Any                      # cases.Case
+    nsteps: int
+    vortex: Optional[dict] = None
+    arrival: float = 0.0           # seconds after the start of the run
+    # filled in by the server
+    admitted: float = math.nan
+    started: float = math.nan      # its cohort began stepping
+    finished: float = math.nan     # results on the host
+    cohort: int = -1
+    result: Optional[np.ndarray] = None
+
+    @property
+    def time_to_forecast(self) -> float:
+        return self.finished - self.arrival
+
+    def node_level_steps(self) -> int:
+        return int(self.case.n_nodes) * int(self.case.vgrid.nvrt) * int(self.nsteps)
+
+
+class ModelEngine:
+    """GPU engine: one batch context (`Model`) per cohort, all stepping on one shared stream."""
+
+    def __init__(self, precision: str = "fp32_ir", device: int = 0, fields: Sequence[str] = ("ETA2",)):
+        import torch
+        from .model import footprint_bytes
+        self.torch = torch
+        self.precision, self.device, self.fields = precision, device, tuple(fields)
+        torch.cuda.set_device(device)
+        self.stream = torch.cuda.Stream(device)
+        self._footprint = footprint_bytes
+
+    def footprint(self, cases) -> int:
+        return self._footprint(cases)
+
+    def free_bytes(self) -> int:
+        return int(self.torch.cuda.mem_get_info(self.device)[0])
+
+    def build(self, reqs: Sequence[Request]):
+        from .model import Model
+        self.torch.cuda.set_device(self.device)
+        m = Model([r.case for r in reqs], precision=self.precision, device=self.device)
+        for i, r in enumerate(reqs):
+            if r.vortex is not None:
+                m.set_vortex(i, r.vortex)
+        m.sync()
+        m.set_stream(self.stream.cuda_stream)
+        return m
+
+    def advance(self, h, k: int) -> None:
+        h.step(k)
+
+    def wait(self) -> None:
+        self.stream.synchronize()
+
+    def results(self, h, n: int) -> List[Dict[str, np.ndarray]]:
+        h.sync()
+        return [{f: h.get(i, f).copy() for f in self.fields} for i in range(n)]
+
+    def close(self, h) -> None:
+        h.close()
+
+
+@dataclasses.dataclass
+class _Cohort:
+    cid: int
+    reqs: List[Request]
+    nbytes: int
+    target: int
+    future: Any = None
+    handle: Any = None
+    done: int = 0
+
+
+class Server:
+    """Continuous-batching scheduler over an engine (see the module docstring)."""
+
+    def __init__(self, engine, budget_bytes: Optional[int] = None, max_members: int = 64,
+                 steps_per_turn: int = 8, background_build: bool = True,
+                 clock: Callable[[], float] = time.perf_counter, sleep: Callable[[float], None] = time.sleep):
+        self.engine = engine
+        self.budget = int(budget_bytes if budget_bytes is not None else 0.9 * engine.free_bytes())
+        self.max_members = max_members
+        self.steps_per_turn = max(1, steps_per_turn)
+        self.clock, self.sleep = clock, sleep
+        self.pool = cf.ThreadPoolExecutor(max_workers=1) if background_build else None
+        self.used = 0
+        self.peak_used = 0
+        self.log: List[tuple] = []
+
+    def _admit(self, queue: List[Request], now: float, cid: int) -> Optional[_Cohort]:
+        """Longest FIFO prefix of same-horizon requests that fits in the free budget."""
+        if not queue:
+            return None
+        group: List[Request] = []
+        nbytes = 0
+        for r in queue:
+            if group and (r.nsteps != group[0].nsteps or r.case.vgrid.nvrt != group[0].case.vgrid.nvrt
+                          or r.case.ntracers != group[0].case.ntracers or r.case.params.dt != group[0].case.params.dt):
+                break
+            if len(group) >= self.max_members:
+                break
+            nb = self.engine.footprint([q.case for q in group + [r]])
+            if self.used + nb > self.budget:
+                break
+            group.append(r)
+            nbytes = nb
+        if not group:
+            if self.used == 0:
+                raise RuntimeError(f"request {queue[0].rid} needs more device memory than the budget")
+            return None
+        del queue[:len(group)]
+        for r in group:
+            r.admitted = now
+            r.cohort = cid
+        self.used += nbytes
+        self.peak_used = max(self.peak_used, self.used)
+        c = _Cohort(cid=cid, reqs=group, nbytes=nbytes, target=group[0].nsteps)
+        if self.pool is not None:
+            c.future = self.pool.submit(self.engine.build, group)
+        else:
+            c.handle = self.engine.build(group)
+        self.log.append(("admit", now, cid, [r.rid for r in group], nbytes))
+        return c
+
+    def run(self, requests: Sequence[Request]) -> List[Request]:
+        pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
+        queue: List[Request] = []
+        building: List[_Cohort] = []
+        active: List[_Cohort] = []
+        t0 = self.clock()
+        cid = 0
+        try:
+            while pending or queue or building or active:
+                now = self.clock() - t0
+                while pending and pending[0].arrival <= now:
+                    queue.append(pending.pop(0))
+                while True:
+                    c = self._admit(queue, now, cid)
+                    if c is None:
+                        break
+                    cid += 1
+                    building.append(c)
+                # cohorts whose build finished join the stepping
+                for c in list(building):
+                    if c.future is not None:
+                        if not c.future.done():
+                            continue
+                        c.handle = c.future.result()
+                    building.remove(c)
+                    active.append(c)
+                    t = self.clock() - t0
+                    for r in c.reqs:
+                        r.started = t
+                if not active:
+                    # nothing to step: wait for a build or the next arrival
+                    waits = []
+                    if pending and not building:
+                        waits.append(pending[0].arrival - now)
+                    self.sleep(max(0.0, min(waits)) if waits else 0.002)
+                    continue
+                for c in active:
+                    k = min(self.steps_per_turn, c.target - c.done)
+                    self.engine.advance(c.handle, k)
+                    c.done += k
+                self.engine.wait()
+                for c in list(active):
+                    if c.done < c.target:
+                        continue
+                    res = self.engine.results(c.handle, len(c.reqs))
+                    t = self.clock() - t0
+                    for r, x in zip(c.reqs, res):
+                        r.result = x
+                        r.finished = t
+                    self.engine.close(c.handle)
+                    active.remove(c)
+                    self.used -= c.nbytes
+                    self.log.append(("finish", t, c.cid))
+        finally:
+            if self.pool is not None:
+                self.pool.shutdown(wait=True)
+        return list(requests)
+
+
+def summary(reqs: Sequence[Request], makespan: float) -> dict:
+    ttf = np.array([r.time_to_forecast for r in reqs])
+    nls = sum(r.node_level_steps() for r in reqs)
+    return {
+        "requests": len(reqs),
+        "ttf_p50_s": float(np.percentile(ttf, 50)),
+        "ttf_p99_s": float(np.percentile(ttf, 99)),
+        "ttf_max_s": float(ttf.max()),
+        "makespan_s": makespan,
+        "node_level_steps_per_s": nls / makespan if makespan > 0 else math.nan,
+        "cohorts": len({r.cohort for r in reqs}),
+    }
+
+
+def poisson_requests(n: int, rate: float, seed: int, hours: float = 48.0, nmin: int = 10_000,
+                     nmax: int = 2_000_000, nvrt: int = 20, dt: float = 150.0) -> List[Request]:
+    """n storm-surge requests (cases.storm) with exponential inter-arrival times of mean 1/rate."""
+    from . import cases
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        if i > 0:
+            t += rng.exponential(1.0 / rate)
+        c, v, nsteps = cases.storm(int(rng.integers(1, 2**31 - 1)), nmin=nmin, nmax=nmax, nvrt=nvrt, dt=dt,
+                                   hours=hours)
+        out.append(Request(rid=i, case=c, nsteps=nsteps, vortex=v, arrival=t))
+    return out
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--requests", type=int, default=16)
+    ap.add_argument("--rate", type=float, default=2.0, help="mean arrivals per second (Poisson)")
+    ap.add_argument("--hours", type=float, default=48.0, help="forecast horizon")
+    ap.add_argument("--nmin", type=int, default=10_000)
+    ap.add_argument("--nmax", type=int, default=2_000_000)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--budget-gb", type=float, default=None)
+    ap.add_argument("--steps-per-turn", type=int, default=8)
+    ap.add_argument("--precision", choices=["fp64", "fp32_ir"], default="fp32_ir")
+    a = ap.parse_args(argv)
+    reqs = poisson_requests(a.requests, a.rate, a.seed, hours=a.hours, nmin=a.nmin, nmax=a.nmax)
+    eng = ModelEngine(precision=a.precision)
+    srv = Server(eng, budget_bytes=None if a.budget_gb is None else int(a.budget_gb * 1e9),
+                 steps_per_turn=a.steps_per_turn)
+    t0 = time.perf_counter()
+    srv.run(reqs)
+    out = summary(reqs, time.perf_counter() - t0)
+    out.update({"horizon_hours": a.hours, "rate_per_s": a.rate, "nodes": [int(r.case.n_nodes) for r in reqs],
+                "ttf_s": [round(r.time_to_forecast, 3) for r in reqs], "peak_budget_gb": srv.peak_used / 1e9})
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -3,7 +3,7 @@
  * One context (gs_ctx) holds a batch of ensemble members (independent meshes of any size that
  * share the vertical grid and the physics constants) resident in the HBM of one GPU.  Every
  * phase of the step runs as one launch over all members; the whole step is a fixed launch
- * sequence on the context's stream, captured once in a CUDA graph.
+ * sequence on the context's stream.
  *
  * Conventions: every entry point returns a gs_status (0 = GS_OK) and never aborts the process;
  * gs_last_error() describes the last failure.  Host pointers are caller-owned and only read
@@ -104,7 +104,7 @@ gs_status gs_sync(gs_ctx* ctx);
  * events recorded on that stream. */
 gs_status gs_set_stream(gs_ctx* ctx, void* stream);
 
-/* Advance every member by nsteps steps (schism_step.py:95-334), as CUDA-graph launches. */
+/* Advance every member by nsteps steps (schism_step.py:95-334). */
 gs_status gs_step(gs_ctx* ctx, int nsteps);
 
 /* Individual phases of one step, in call order (the cufunc kernels of schism_step.py). */
@@ -127,6 +127,7 @@ gs_status gs_phase(gs_ctx* ctx, int phase, int arg);
 enum {
     GS_F_ETA1 = 0, GS_F_ETA2 = 1, GS_F_NODE_Z = 2, GS_F_NODE_U2 = 3, GS_F_NODE_W2 = 4,
     GS_F_NODE_TR = 5, GS_F_NODE_KB = 6, GS_F_NODE_DRY = 7, GS_F_QEL = 8,
+    GS_F_NODE_TAU = 9,                   /* surface stress [np][2] (kinematic) */
     GS_F_SIDE_U2 = 10, GS_F_SIDE_BTU = 11, GS_F_SIDE_ZC = 12, GS_F_SIDE_KB = 13, GS_F_SIDE_DRY = 14,
     GS_F_SIDE_U = 15, GS_F_SIDE_HHAT = 16, GS_F_SIDE_CHI = 17, GS_F_SIDE_QH = 18,
     GS_F_SIDE_BTELEM = 19, GS_F_SIDE_GRADETA1 = 20, GS_F_SIDE_GRADETA2 = 21,
@@ -140,6 +141,28 @@ gs_status gs_state_get(gs_ctx* ctx, int member, int field, void* host, size_t by
 gs_status gs_state_put(gs_ctx* ctx, int member, int field, const void* host, size_t bytes);
 /* Per-step host forcing: replace a member's surface stress [np][2] (host buffer, copied). */
 gs_status gs_set_tau(gs_ctx* ctx, int member, const double* tau_host);
+
+/* Parametric storm forcing for a member (storm-surge scenarios): a radial vortex moving along a
+   straight track, evaluated on the device at the start of every step.  Wind speed at distance r
+   from the centre W(r) = vmax * sqrt((rmax/r)^B exp(1 - (rmax/r)^B)) (Holland profile, W(rmax) =
+   vmax), counter-clockwise, plus the track velocity weighted by W/vmax; drag coefficient
+   1e-3 (0.75 + 0.067 |W|), at most 3e-3; the member's surface stress (kinematic, per node) becomes
+   rho_air/rho0 * Cd |W| W times the step's ramp.  No counterpart in the reference, whose wind comes
+   from forcing files; this generates the synthetic input on the device.  NULL switches it off
+   (the stress set by gs_set_tau / the member description is used again). */
+typedef struct {
+    double x0, y0;        /* centre at time 0 (m, mesh coordinates) */
+    double heading;       /* direction of motion (radians from +x, counter-clockwise) */
+    double speed;         /* translation speed (m/s) */
+    double vmax, rmax;    /* maximum wind (m/s) and its radius (m) */
+    double holland_b;     /* profile shape B (typically 1..2.5) */
+    double rho_air;       /* air density (kg/m^3) */
+} gs_vortex;
+gs_status gs_set_vortex(gs_ctx* ctx, int member, const gs_vortex* vortex);
+
+/* Device memory a context holding members of these sizes allocates (bytes, an upper bound used
+   for admission by HBM footprint).  np/ne/ns/nnz are the sums over the members. */
+size_t gs_footprint_bytes(int nvrt, int ntr, int nmem, int64_t np, int64_t ne, int64_t ns, int64_t nnz);
 
 typedef struct {
     int64_t jcg_iters;         /* iterations of the last solve (inner FP32 iterations for IR) */

@@ -14,6 +14,7 @@ static void* fptr(const og_model* m, int f, fdesc* d) {
     case OGF_ETA1: d->n = m->np; return m->eta1;
     case OGF_ETA2: d->n = m->np; return m->eta2;
     case OGF_QEL: d->n = m->np; return m->qel;
+    case OGF_NODE_TAU: d->n = m->np; d->comp = 2; return m->tau;
     case OGF_ELBC: d->n = m->np; return m->elbc;
     case OGF_JCG_X: d->n = m->np; return m->x0;
     case OGF_JCG_X1: d->n = m->np; return m->x1;

@@ -39,7 +39,7 @@ typedef struct {
  * last for vectors, tracers [ntr][nvrt][n]).  The CUDA product uses the same numbers. */
 enum {
     OGF_ETA1 = 0, OGF_ETA2 = 1, OGF_NODE_Z = 2, OGF_NODE_U2 = 3, OGF_NODE_W2 = 4,
-    OGF_NODE_TR = 5, OGF_NODE_KB = 6, OGF_NODE_DRY = 7, OGF_QEL = 8,
+    OGF_NODE_TR = 5, OGF_NODE_KB = 6, OGF_NODE_DRY = 7, OGF_QEL = 8, OGF_NODE_TAU = 9,
     OGF_SIDE_U2 = 10, OGF_SIDE_BTU = 11, OGF_SIDE_ZC = 12, OGF_SIDE_KB = 13, OGF_SIDE_DRY = 14,
     OGF_SIDE_U = 15, OGF_SIDE_HHAT = 16, OGF_SIDE_CHI = 17, OGF_SIDE_QH = 18,
     OGF_SIDE_BTELEM = 19, OGF_SIDE_GRADETA1 = 20, OGF_SIDE_GRADETA2 = 21,
@@ -60,6 +60,8 @@ int og_put(og_model* m, int field, const void* in);
 
 /* phases of the step (schism_step.py:95-334), callable one by one for parity tests */
 void og_begin_step(og_model* m, int it);                       /* time ramps, forcing */
+/* storm forcing: p = {x0, y0, heading, speed, vmax, rmax, B, rho_air}, NULL = off (stress kept) */
+void og_set_vortex(og_model* m, const double* p);
 void og_btrack(og_model* m);                                   /* mdc:3547-3660 */
 void og_prepare_elevation(og_model* m, double time);           /* BCs, U, hhat/chi, ghat1 */
 void og_assemble(og_model* m, double time);                    /* mdc:3182-3474 */

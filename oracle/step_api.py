@@ -13,7 +13,7 @@ PD = ctypes.POINTER(ctypes.c_double)
 PI = ctypes.POINTER(ctypes.c_int32)
 
 # field codes shared with the product (include/gschism_b200.h, GS_F_*)
-F = dict(ETA1=0, ETA2=1, NODE_Z=2, NODE_U2=3, NODE_W2=4, NODE_TR=5, NODE_KB=6, NODE_DRY=7, QEL=8,
+F = dict(ETA1=0, ETA2=1, NODE_Z=2, NODE_U2=3, NODE_W2=4, NODE_TR=5, NODE_KB=6, NODE_DRY=7, QEL=8, NODE_TAU=9,
          SIDE_U2=10, SIDE_BTU=11, SIDE_ZC=12, SIDE_KB=13, SIDE_DRY=14, SIDE_U=15, SIDE_HHAT=16,
          SIDE_CHI=17, SIDE_QH=18, SIDE_BTELEM=19, SIDE_GRADETA1=20, SIDE_GRADETA2=21,
          ELEM_Z=30, ELEM_W=31, ELEM_QV=32, ELEM_TR=33, ELEM_KB=34, ELEM_DRY=35, ELEM_GHAT=36,
@@ -63,6 +63,7 @@ def declare(L) -> None:
     L.og_counters.argtypes = [c_void_p, ctypes.POINTER(ctypes.c_int64)]
     L.og_tracer_mass.argtypes = [c_void_p, PD]
     L.og_set_solver.argtypes = [c_void_p, c_double, c_int, c_int]
+    L.og_set_vortex.argtypes = [c_void_p, PD]
 
 
 def _pd(a):
@@ -124,6 +125,16 @@ class OracleModel:
                              int(maxiter if maxiter is not None else p.maxiter),
                              int(check_every if check_every is not None else p.check_every))
 
+    VORTEX_KEYS = ("x0", "y0", "heading", "speed", "vmax", "rmax", "holland_b", "rho_air")
+
+    def set_vortex(self, vortex) -> None:
+        """Storm forcing (og_set_vortex), same parameters as the product's gs_vortex; None = off."""
+        if vortex is None:
+            self.L.og_set_vortex(self.h, None)
+            return
+        self._vortex = np.array([float(vortex[k]) for k in self.VORTEX_KEYS], dtype=np.float64)
+        self.L.og_set_vortex(self.h, _pd(self._vortex))
+
     def __del__(self):
         try:
             if getattr(self, "h", None):
@@ -142,6 +153,8 @@ class OracleModel:
             return (n[per[name][0]],)
         if name in ("SIDE_U", "SIDE_GRADETA1", "SIDE_GRADETA2"):
             return (self.ns, 2)
+        if name == "NODE_TAU":
+            return (self.np, 2)
         if name == "ELEM_GHAT":
             return (self.ne, 2)
         if name in ("NODE_Z", "NODE_W2"):

@@ -32,6 +32,7 @@ struct og_model {
     double *amig, *ff, *face;
     /* nodes */
     double *x, *y, *depth, *drag, *Cd, *grav2, *tau, *eta1, *eta2, *qel, *mX, *elbc;
+    double vortex[8]; int has_vortex;   /* storm forcing (og_set_vortex) */
     int32_t* kb; uint8_t *ndry, *nwas, *ess;
     double* z; v2* u2; double* w2; double* tr; double* tr_init;
     double *nbfr_emo, *nbfr_efa;
