@@ -105,6 +105,7 @@ struct Dev {
     double *mem_scal;              // per member scalars (see jcg.cu)
     int32_t *mem_iters, *mem_outer;
     // global control
+    double* clk;                   // [3] step, time = step * dt, ramp (set on the device each step)
     unsigned* bar;                  // grid barrier word (zero between launches)
     int32_t *err;
     unsigned long long *counters;  // [4]: walk cap hits, btrack stops, ...

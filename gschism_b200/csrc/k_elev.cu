@@ -10,8 +10,20 @@
 
 namespace gs {
 
-__global__ void k_elev_bc(Dev d, double time, double ramp) {
+// Step clock on the device (computeTimeRamps, mdh:2036-2077): step index, time and the tanh
+// ramp, so the step's launch sequence has no per-step host arguments and replays as a graph.
+__device__ __forceinline__ void clock_at(Dev& d, const Phys& P, int it) {
+    const double time = it * P.dt;
+    d.clk[0] = it;
+    d.clk[1] = time;
+    d.clk[2] = (P.dramp > 0.0) ? tanh(2.0 * time / 86400.0 / P.dramp) : 1.0;
+}
+__global__ void k_clock_set(Dev d, Phys P, int it) { clock_at(d, P, it); }
+__global__ void k_clock_advance(Dev d, Phys P) { clock_at(d, P, (int)d.clk[0] + 1); }
+
+__global__ void k_elev_bc(Dev d) {
     // computeElevationBoundaryConditions, mdc:4276-4339 (iettype 3: tidal harmonics)
+    const double time = d.clk[1], ramp = d.clk[2];
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < d.NB; b += gridDim.x * blockDim.x) {
         const int i = d.bn_node[b];
         const int iettype = d.bn_ietype[b];
@@ -227,7 +239,8 @@ __global__ void k_update_elev(Dev d, VG vg) {
 
 // Storm forcing: kinematic surface stress of a radial vortex on a straight track (gs_vortex in the
 // C ABI) for the nodes of members that have one; other members keep their stress.
-__global__ void k_vortex_tau(Dev d, double time, double ramp, double rho0) {
+__global__ void k_vortex_tau(Dev d, double rho0) {
+    const double time = d.clk[1], ramp = d.clk[2];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.NP; i += gridDim.x * blockDim.x) {
         int lo = 0, hi = d.nmem;                       // member of node i: mem_np0[lo] <= i < mem_np0[lo+1]
         while (hi - lo > 1) {
@@ -258,9 +271,12 @@ __global__ void k_vortex_tau(Dev d, double time, double ramp, double rho0) {
     }
 }
 
-void launch_elev_prepare(const Dev& d, const Phys& P, double time, double ramp, bool vortex, cudaStream_t st, int nsm) {
-    if (vortex) k_vortex_tau<<<grid_for(d.NP, 256, nsm * 8), 256, 0, st>>>(d, time, ramp, P.rho0);
-    if (d.NB > 0) k_elev_bc<<<grid_for(d.NB, 128, nsm * 4), 128, 0, st>>>(d, time, ramp);
+void launch_clock_set(const Dev& d, const Phys& P, int it, cudaStream_t st) { k_clock_set<<<1, 1, 0, st>>>(d, P, it); }
+void launch_clock_advance(const Dev& d, const Phys& P, cudaStream_t st) { k_clock_advance<<<1, 1, 0, st>>>(d, P); }
+
+void launch_elev_prepare(const Dev& d, const Phys& P, bool vortex, cudaStream_t st, int nsm) {
+    if (vortex) k_vortex_tau<<<grid_for(d.NP, 256, nsm * 8), 256, 0, st>>>(d, P.rho0);
+    if (d.NB > 0) k_elev_bc<<<grid_for(d.NB, 128, nsm * 4), 128, 0, st>>>(d);
     k_side_prep<<<grid_for(d.NS, 256, nsm * 16), 256, 0, st>>>(d, P);
     k_ghat<<<grid_for(d.NE, 256, nsm * 16), 256, 0, st>>>(d, P);
 }

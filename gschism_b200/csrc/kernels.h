@@ -35,7 +35,9 @@ cudaError_t jcg_read_iters(JcgWork* w, std::vector<int>& iters, std::vector<int>
 int32_t* jcg_iters_device(JcgWork* w);
 
 // k_elev.cu
-void launch_elev_prepare(const Dev& d, const Phys& P, double time, double ramp, bool vortex, cudaStream_t st, int nsm);
+void launch_clock_set(const Dev& d, const Phys& P, int it, cudaStream_t st);
+void launch_clock_advance(const Dev& d, const Phys& P, cudaStream_t st);
+void launch_elev_prepare(const Dev& d, const Phys& P, bool vortex, cudaStream_t st, int nsm);
 void launch_assemble(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
 void launch_update_elev(const Dev& d, const VG& vg, cudaStream_t st, int nsm);
 // k_btrack.cu

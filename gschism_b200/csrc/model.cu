@@ -64,8 +64,10 @@ struct gs_ctx {
     JcgWork* jw = nullptr;
     std::vector<void*> allocs;
     int it = 0;
+    // gs_step replays one captured step; recaptured when storm forcing switches on or off
     cudaGraphExec_t graph = nullptr;
-    int32_t* d_it = nullptr;
+    int graph_vortex = -1;
+    bool graph_failed = false;       // capture refused: gs_step launches the phases directly
     std::string err;
     std::vector<int> last_iters, last_outer;
     // batch CSR of the elevation matrix on the host (export) and each CSR entry's SELL position
@@ -457,7 +459,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     c->h_vort.assign((size_t)kVortexParams * c->mem.size(), 0.0);
     UP(vort, c->h_vort);
     AL(mem_rem, 2 * (size_t)d.nmem); AL(mem_dtb, d.nmem); AL(mem_mindt, 2 * (size_t)d.nmem + 1); AL(mem_nsub, d.nmem);
-    AL(bar, 1); AL(err, 1); AL(counters, 4);
+    AL(clk, 3); AL(bar, 1); AL(err, 1); AL(counters, 4);
 #undef UP
 #undef AL
     if (e != cudaSuccess) return c->fail(e == cudaErrorMemoryAllocation ? GS_ERR_OOM : GS_ERR_CUDA, cudaGetErrorString(e));
@@ -496,18 +498,13 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
 
 // ------------------------------------------------------------------------- phases ----
 
-static double ramp_of(const gs_ctx* c, double time) {
-    return (c->cfg.dramp > 0.0) ? std::tanh(2.0 * time / 86400.0 / c->cfg.dramp) : 1.0;
-}
-
 static gs_status run_phase(gs_ctx* c, int phase, int arg) {
     const int nsm = c->nsm;
     cudaStream_t st = c->st;
-    const double time = c->it * c->cfg.dt;
     switch (phase) {
-    case GS_PHASE_BEGIN: c->it = arg; break;
+    case GS_PHASE_BEGIN: c->it = arg; launch_clock_set(c->d, c->P, arg, st); break;
     case GS_PHASE_BTRACK: launch_btrack(c->d, c->P, c->vg, st, nsm); break;
-    case GS_PHASE_PREPARE: launch_elev_prepare(c->d, c->P, time, ramp_of(c, time), c->nvortex > 0, st, nsm); break;
+    case GS_PHASE_PREPARE: launch_elev_prepare(c->d, c->P, c->nvortex > 0, st, nsm); break;
     case GS_PHASE_ASSEMBLE:
         launch_assemble(c->d, c->P, st, nsm);
         break;
@@ -562,18 +559,60 @@ gs_status gs_phase(gs_ctx* c, int phase, int arg) {
     return run_phase(c, phase, arg);
 }
 
+}  // extern "C"
+
+// One step as a fixed launch sequence: advance the device clock, then every phase.  The LEVELS
+// phase only tells the cold start (step 0) from a step, so any step index >= 1 gives the same
+// launches.
+static gs_status launch_step(gs_ctx* c) {
+    launch_clock_advance(c->d, c->P, c->st);
+    const int seq[] = {GS_PHASE_BTRACK, GS_PHASE_PREPARE, GS_PHASE_ASSEMBLE, GS_PHASE_SOLVE, GS_PHASE_UPDATE_ELEV,
+                       GS_PHASE_MOMENTUM, GS_PHASE_VVEL, GS_PHASE_TRANSPORT, GS_PHASE_LEVELS, GS_PHASE_NODAL_VEL};
+    for (int ph : seq) {
+        const gs_status s = run_phase(c, ph, 1);
+        if (s != GS_OK) return s;
+    }
+    return GS_OK;
+}
+
+// Capture one step into a CUDA graph (once, and again when storm forcing switches on or off).
+// A refused capture leaves gs_step on direct launches.
+static void ensure_graph(gs_ctx* c) {
+    const int vort = c->nvortex > 0 ? 1 : 0;
+    if (c->graph_failed || (c->graph && c->graph_vortex == vort)) return;
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+    gs_status s = GS_OK;
+    if (e == cudaSuccess) {
+        s = launch_step(c);
+        e = cudaStreamEndCapture(c->st, &g);
+    }
+    if (e == cudaSuccess && s == GS_OK) e = cudaGraphInstantiate(&c->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess || s != GS_OK) {
+        c->graph = nullptr;
+        c->graph_failed = true;
+        cudaGetLastError();
+        return;
+    }
+    c->graph_vortex = vort;
+}
+
+extern "C" {
+
 gs_status gs_step(gs_ctx* c, int nsteps) {
     if (!c || !c->finalized || nsteps < 0) return GS_ERR_ARG;
+    if (nsteps > 0) ensure_graph(c);
     for (int n = 0; n < nsteps; n++) {
-        const int it = c->it + 1;
-        const int seq[] = {GS_PHASE_BTRACK, GS_PHASE_PREPARE, GS_PHASE_ASSEMBLE, GS_PHASE_SOLVE, GS_PHASE_UPDATE_ELEV,
-                           GS_PHASE_MOMENTUM, GS_PHASE_VVEL, GS_PHASE_TRANSPORT, GS_PHASE_LEVELS, GS_PHASE_NODAL_VEL};
-        gs_status s = run_phase(c, GS_PHASE_BEGIN, it);
-        for (int ph : seq) {
+        if (c->graph) {
+            const cudaError_t e = cudaGraphLaunch(c->graph, c->st);
+            if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, std::string("step graph: ") + cudaGetErrorString(e));
+        } else {
+            const gs_status s = launch_step(c);
             if (s != GS_OK) return s;
-            s = run_phase(c, ph, it);
         }
-        if (s != GS_OK) return s;
+        c->it++;
     }
     return GS_OK;
 }
@@ -620,8 +659,8 @@ gs_status gs_get_stats(gs_ctx* c, int member, gs_stats* out) {
 
 gs_status gs_ctx_destroy(gs_ctx* c) {
     if (!c) return GS_ERR_ARG;
-    if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->st) cudaStreamSynchronize(c->st);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->own_st) cudaStreamDestroy(c->own_st);
     jcg_work_free(c->jw);
     for (void* p : c->allocs) cudaFree(p);

@@ -3,7 +3,7 @@
  * One context (gs_ctx) holds a batch of ensemble members (independent meshes of any size that
  * share the vertical grid and the physics constants) resident in the HBM of one GPU.  Every
  * phase of the step runs as one launch over all members; the whole step is a fixed launch
- * sequence on the context's stream.
+ * sequence on the context's stream, which gs_step captures once in a CUDA graph and replays.
  *
  * Conventions: every entry point returns a gs_status (0 = GS_OK) and never aborts the process;
  * gs_last_error() describes the last failure.  Host pointers are caller-owned and only read
@@ -104,7 +104,10 @@ gs_status gs_sync(gs_ctx* ctx);
  * events recorded on that stream. */
 gs_status gs_set_stream(gs_ctx* ctx, void* stream);
 
-/* Advance every member by nsteps steps (schism_step.py:95-334). */
+/* Advance every member by nsteps steps (schism_step.py:95-334): replays of one captured step
+ * (a CUDA graph; the step clock, time and ramp live on the device).  The first call captures it,
+ * and again after gs_set_vortex switches storm forcing on or off for the first/last member;
+ * it must therefore not be made while the stream is being captured by the caller. */
 gs_status gs_step(gs_ctx* ctx, int nsteps);
 
 /* Individual phases of one step, in call order (the cufunc kernels of schism_step.py). */

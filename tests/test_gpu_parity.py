@@ -151,3 +151,29 @@ def test_mixed_precision_elevation_within_1e6_m(native, oracle_lib):
     assert err <= 1e-6, err
     st = g.stats(0)
     assert st["jcg_outer"] >= 1
+
+
+def test_graph_step_equals_phase_by_phase(native):
+    """gs_step (one captured step replayed as a CUDA graph) gives the same bits as the same
+    steps issued phase by phase, also across a recapture when storm forcing switches on."""
+    from gschism_b200.model import Model
+    c, v, _ = cases.storm(41, nmin=2500, nmax=2500, hours=1.0)
+    a, b = Model([c]), Model([c])
+    phases = ["BTRACK", "PREPARE", "ASSEMBLE", "SOLVE", "UPDATE_ELEV", "MOMENTUM", "VVEL", "TRANSPORT",
+              "LEVELS", "NODAL_VEL"]
+
+    def by_phase(m, it):
+        m.phase("BEGIN", it)
+        for ph in phases:
+            m.phase(ph, it)
+
+    a.step(3)
+    for it in range(1, 4):
+        by_phase(b, it)
+    a.set_vortex(0, v)
+    b.set_vortex(0, v)
+    a.step(3)
+    for it in range(4, 7):
+        by_phase(b, it)
+    for f in ("ETA2", "SIDE_U2", "ELEM_TR", "NODE_TAU"):
+        assert np.array_equal(a.get(0, f), b.get(0, f)), f
