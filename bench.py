@@ -139,13 +139,14 @@ def run_ours(a):
     import torch
     from gschism_b200 import cases
     from gschism_b200.model import Model
+    from gschism_b200.shard import max_over_ranks
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
     dist = None
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     case = cases.basin(seed=2 + 0, n=a.n, nvrt=30, nz=10, ntr=2)
     nodes, nvrt = case.n_nodes, case.nvrt
     res = {}
@@ -186,10 +187,7 @@ def run_ours(a):
         jms = [s.elapsed_time(e) for s, e in jev]
         st = m.stats(0)
         m.sync()
-        t = torch.tensor([ms], device="cuda")
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+        ms_max = max_over_ranks(ms, dist, device="cuda")
         total = nodes * nvrt * a.steps * ws
         res[mode] = dict(value=total / (ms_max / 1e3), ms_per_step=ms_max / a.steps, jcg_ms=jms, stats=st,
                          clocks=clk.summary(), nnz=m.sizes[0]["nnz"])
@@ -213,10 +211,7 @@ def run_ours(a):
             torch.cuda.synchronize()
             wall = time.perf_counter() - t0
             ems = max(e0.elapsed_time(e1), wall * 1e3)
-            te = torch.tensor([ems], device="cuda")
-            if dist is not None:
-                dist.all_reduce(te, op=dist.ReduceOp.MAX)
-            res[mode]["e2e"] = dict(value=total / (float(te.item()) / 1e3), unit=METRIC,
+            res[mode]["e2e"] = dict(value=total / (max_over_ranks(ems, dist, device="cuda") / 1e3), unit=METRIC,
                                     h2d_bytes_per_step=int(tau.nbytes), d2h_bytes_per_step=int(eta.nbytes))
         m.close()
         del m
