@@ -165,92 +165,6 @@ __device__ __forceinline__ bool checkpoint(const JcgView& J, int it, int maxit) 
     return ((it + 1) % J.check_every == 0) || (it == maxit - 1);
 }
 
-// ---------------------------------------------------------------- one CG iteration (templated)
-
-// Phase A of CG iteration `it` on the tiles of this block.  T = double (FP64 solve) or float
-// (inner solve of the refinement).  Members whose iteration it-1 met the tolerance at a
-// checkpoint are retired here (the member's first tile records the count).
-template <bool SELL, typename T>
-__device__ void cg_phase_a(const JcgView& J, int it, int maxit, const T* A, const T* z, T* pc, T* pn, T* q,
-                           double* sh, int* shv) {
-    const int tid = threadIdx.x;
-    const int cur = (it + 1) & 1, old = it & 1;
-    const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
-    int cm = -1;
-    bool active = false;
-    double beta = 0.0;
-    for (int t = tb0; t < tb1; t++) {
-        const int m = J.tile_mem[t];
-        if (m != cm) {
-            cm = m;
-            active = uniform_ld(&J.mdone[m], shv) < 0;
-            if (active) {
-                const int kinds[3] = {cur ? R_RR1 : R_RR0, cur ? R_RZ1 : R_RZ0, old ? R_RZ1 : R_RZ0};
-                double tot[3];
-                member_totals<3>(J, m, kinds, tot, sh);
-                if (it > 0 && checkpoint(J, it - 1, maxit) && tot[0] <= J.mem_atol2[m]) {
-                    active = false;
-                    if (t == J.mem_t0[m] && tid == 0) { J.mdone[m] = it; __threadfence(); atomicAdd(J.ndone, 1u); }
-                } else {
-                    beta = (it == 0 || tot[2] == 0.0) ? 0.0 : tot[1] / tot[2];
-                }
-            }
-        }
-        if (!active) continue;
-        const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
-        double v[1] = {0.0};
-        const T bt = (T)beta;
-        for (int i = r0 + tid; i < r1; i += kThreads) {
-            const T s = row_dot<SELL, T>(J, A, i, [&](int c) { return z[c] + bt * pc[c]; });
-            const T pi = z[i] + bt * pc[i];
-            pn[i] = pi; q[i] = s;
-            v[0] += (double)pi * (double)s;
-        }
-        const int kinds[1] = {R_PQ};
-        put_partials<1>(J, t, kinds, v, sh);
-    }
-}
-
-// Phase B of iteration it: x += alpha p; r -= alpha q; z = invD r; (r.r, r.z) partials.
-template <typename T>
-__device__ void cg_phase_b(const JcgView& J, int it, int maxit, T* x, T* r, T* z, const T* pn, const T* q,
-                           const T* invD, double* sh, int* shv) {
-    const int tid = threadIdx.x;
-    const int cur = (it + 1) & 1;
-    const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
-    const int srr = (it & 1) ? R_RR1 : R_RR0, srz = (it & 1) ? R_RZ1 : R_RZ0;
-    int cm = -1;
-    bool active = false;
-    double alpha = 0.0;
-    for (int t = tb0; t < tb1; t++) {
-        const int m = J.tile_mem[t];
-        if (m != cm) {
-            cm = m;
-            active = uniform_ld(&J.mdone[m], shv) < 0;
-            if (active) {
-                const int kinds[3] = {R_PQ, cur ? R_RZ1 : R_RZ0, cur ? R_RR1 : R_RR0};
-                double tot[3];
-                member_totals<3>(J, m, kinds, tot, sh);
-                if (it > 0 && checkpoint(J, it - 1, maxit) && tot[2] <= J.mem_atol2[m]) active = false;
-                else alpha = (tot[0] != 0.0) ? tot[1] / tot[0] : 0.0;
-            }
-        }
-        if (!active) continue;
-        const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
-        const T al = (T)alpha;
-        double v[2] = {0.0, 0.0};
-        for (int i = r0 + tid; i < r1; i += kThreads) {
-            x[i] += al * pn[i];
-            const T ri = r[i] - al * q[i];
-            const T zi = invD[i] * ri;
-            r[i] = ri; z[i] = zi;
-            v[0] += (double)ri * (double)ri; v[1] += (double)ri * (double)zi;
-        }
-        const int kinds[2] = {srr, srz};
-        put_partials<2>(J, t, kinds, v, sh);
-    }
-}
-
 // |b|^2 partials (and zero the search directions of both precisions)
 __device__ void phase_bb(const JcgView& J, double* sh) {
     const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
@@ -287,25 +201,121 @@ __device__ void phase_atol(const JcgView& J, double* sh) {
 #define GSYNC() do { if (!grid_sync(J.bar, J.err)) return; } while (0)
 
 // ------------------------------------------------------------------------------- FP64 ----
+//
+// The reference's two-phase iteration with member-level synchronisation instead of grid
+// barriers (as the FP32 solve, below): after its tiles of member m a block adds one to mcnt[m];
+// the member's last arriver sums the member's partials in tile order and publishes the scalar
+// the next phase needs in mpub[2m] (alpha) or mpub[2m+1] (beta), with mgen[m] = 2 it + 2 (alpha of
+// iteration it) or 2 it + 3 (beta of iteration it + 1); mgen = 0 means nothing published yet and
+// kRetired a finished member.  The totals, and so alpha, beta, the iterates and the iteration
+// counts, are those of the grid-barrier form bit for bit.
+
+constexpr int kRetired64 = 0x7fffffff;
+
+__device__ __forceinline__ int ld_acquire_s32(const int32_t* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Wait until member m has published generation g.  Returns the published scalar in *val and
+// 1 = on, 0 = finished, -1 = failed (bounded) wait.
+__device__ __forceinline__ int wait64(const JcgView& J, int m, int g, int slot, double* shd, int* shv) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long spins = 0;
+        int cur, st = 1;
+        while ((cur = ld_acquire_s32(&J.mgen[m])) < g) {
+            if (++spins > 4096) __nanosleep(128);
+            if (spins > (1ll << 24)) { atomicOr(J.err, ERR_BARRIER_TIMEOUT); st = -1; break; }
+            if ((spins & 255) == 0 && (*((volatile int32_t*)J.err) & ERR_BARRIER_TIMEOUT)) { st = -1; break; }
+        }
+        __threadfence();
+        if (st == 1 && cur == kRetired64) st = 0;
+        if (st == 1) *shd = __ldcg(&J.mpub[2 * m + slot]);
+        *shv = st;
+    }
+    __syncthreads();
+    return *shv;
+}
+
+__device__ __forceinline__ void publish64(const JcgView& J, int m, int g, int slot, double val) {
+    J.mpub[2 * m + slot] = val;
+    __threadfence();
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(&J.mgen[m]), "r"(g) : "memory");
+}
+
+// Arrival of this block at member m; returns true in the whole block for the last arriver.
+__device__ __forceinline__ bool arrive64(const JcgView& J, int m, int* shv) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned old = atomicAdd(&J.mcnt[m], 1u);
+        const bool last = ((old + 1u) % (unsigned)J.mnblk[m]) == 0u;
+        if (last) __threadfence();
+        *shv = last ? 1 : 0;
+    }
+    __syncthreads();
+    return *shv != 0;
+}
+
+// Scalars of phase A of iteration nit (nit >= 1) from the partials of iteration nit - 1's phase B,
+// published by the member's last arriver: the checkpoint test, then beta.
+__device__ void publish_beta(const JcgView& J, int m, int nit, double* sh) {
+    const int cur = (nit + 1) & 1, old = nit & 1;
+    const int kinds[3] = {cur ? R_RR1 : R_RR0, cur ? R_RZ1 : R_RZ0, old ? R_RZ1 : R_RZ0};
+    double tot[3];
+    member_totals<3>(J, m, kinds, tot, sh);
+    if (threadIdx.x != 0) return;
+    if (checkpoint(J, nit - 1, J.maxiter) && tot[0] <= J.mem_atol2[m]) {
+        J.mdone[m] = nit;
+        __threadfence();
+        atomicAdd(J.ndone, 1u);
+        publish64(J, m, kRetired64, 1, 0.0);
+        return;
+    }
+    if (nit == J.maxiter) {
+        // still active after the last iteration: the reference returns maxiter
+        J.mdone[m] = J.maxiter;
+        atomicOr(J.err, ERR_JCG_NOT_CONVERGED);
+        __threadfence();
+        atomicAdd(J.ndone, 1u);
+        publish64(J, m, kRetired64, 1, 0.0);
+        return;
+    }
+    publish64(J, m, 2 * nit + 1, 1, (tot[2] == 0.0) ? 0.0 : tot[1] / tot[2]);
+}
 
 template <bool SELL>
 __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
     __shared__ double sh[4 * 32];
+    __shared__ double shd;
     __shared__ int shv;
+    const int tid = threadIdx.x;
+    const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
     phase_bb(J, sh);
     GSYNC();
     phase_atol(J, sh);
     GSYNC();
-    // r = b - A x; z = invD r; (r.r, r.z) into the parity-1 slots (iteration -1)
+    // r = b - A x; z = invD r; (r.r, r.z) into the parity-1 slots (iteration -1); iteration 0 of
+    // a member starts with beta = 0 once all its blocks are here
     {
-        const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
+        int cm = -1;
+        bool on = false;
         for (int t = tb0; t < tb1; t++) {
             const int m = J.tile_mem[t];
-            const bool zero = uniform_ld(&J.mdone[m], &shv) == 0;
+            if (m != cm) {
+                if (cm >= 0 && on && arrive64(J, cm, &shv) && tid == 0) publish64(J, cm, 1, 1, 0.0);
+                cm = m;
+                on = uniform_ld(&J.mdone[m], &shv) < 0;
+            }
             const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
+            if (!on) {
+                for (int i = r0 + tid; i < r1; i += kThreads) { J.x[i] = 0.0; J.r[i] = 0.0; J.z[i] = 0.0; }
+                continue;
+            }
             double v[2] = {0.0, 0.0};
-            for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
-                if (zero) { J.x[i] = 0.0; J.r[i] = 0.0; J.z[i] = 0.0; continue; }
+            for (int i = r0 + tid; i < r1; i += kThreads) {
                 const double s = row_dot<SELL, double>(J, J.A, i, [&](int c) { return J.x[c]; });
                 const double ri = J.b[i] - s, zi = J.invD[i] * ri;
                 J.r[i] = ri; J.z[i] = zi;
@@ -314,27 +324,93 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
             const int kinds[2] = {R_RR1, R_RZ1};
             put_partials<2>(J, t, kinds, v, sh);
         }
+        if (cm >= 0 && on && arrive64(J, cm, &shv) && tid == 0) publish64(J, cm, 1, 1, 0.0);
     }
-    GSYNC();
-    int it = 0;
-    for (; it < J.maxiter; it++) {
-        double* pc = (it & 1) ? J.p1 : J.p0;
+    for (int it = 0; it < J.maxiter; it++) {
+        const double* pc = (it & 1) ? J.p1 : J.p0;
         double* pn = (it & 1) ? J.p0 : J.p1;
-        cg_phase_a<SELL, double>(J, it, J.maxiter, J.A, J.z, pc, pn, J.q, sh, &shv);
-        GSYNC();
-        if (*((volatile unsigned*)J.ndone) >= (unsigned)J.nmem) break;
-        cg_phase_b<double>(J, it, J.maxiter, J.x, J.r, J.z, pn, J.q, J.invD, sh, &shv);
-        GSYNC();
-    }
-    if (it == J.maxiter) {
-        // members still active after the last iteration: the reference returns maxiter
-        const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
-        for (int t = tb0; t < tb1; t++) {
-            const int m = J.tile_mem[t];
-            if (t == J.mem_t0[m] && threadIdx.x == 0 && ld_done(J, m) < 0) {
-                J.mdone[m] = J.maxiter;
-                atomicOr(J.err, ERR_JCG_NOT_CONVERGED);
+        const int cur = (it + 1) & 1;
+        bool any = false;
+        // phase A: p_new = z + beta p; q = A p_new; p.q partials; the last arriver publishes alpha
+        {
+            int cm = -1;
+            bool on = false;
+            double beta = 0.0;
+            for (int t = tb0; t < tb1; t++) {
+                const int m = J.tile_mem[t];
+                if (m != cm) {
+                    if (cm >= 0 && on && arrive64(J, cm, &shv)) {
+                        const int kinds[2] = {R_PQ, cur ? R_RZ1 : R_RZ0};
+                        double tot[2];
+                        member_totals<2>(J, cm, kinds, tot, sh);
+                        if (tid == 0) publish64(J, cm, 2 * it + 2, 0, (tot[0] != 0.0) ? tot[1] / tot[0] : 0.0);
+                    }
+                    cm = m;
+                    on = false;
+                    // a member with mdone >= 0 (zero right-hand side, or retired) publishes no
+                    // more; either value of mdone a block reads leads to the same decision
+                    if (uniform_ld(&J.mdone[m], &shv) < 0) {
+                        const int st = wait64(J, m, 2 * it + 1, 1, &shd, &shv);
+                        if (st < 0) return;
+                        on = st == 1;
+                        beta = (it == 0) ? 0.0 : shd;
+                    }
+                }
+                if (!on) continue;
+                any = true;
+                const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
+                double v[1] = {0.0};
+                for (int i = r0 + tid; i < r1; i += kThreads) {
+                    const double s = row_dot<SELL, double>(J, J.A, i, [&](int c) { return J.z[c] + beta * pc[c]; });
+                    const double pi = J.z[i] + beta * pc[i];
+                    pn[i] = pi; J.q[i] = s;
+                    v[0] += pi * s;
+                }
+                const int kinds[1] = {R_PQ};
+                put_partials<1>(J, t, kinds, v, sh);
             }
+            if (cm >= 0 && on && arrive64(J, cm, &shv)) {
+                const int kinds[2] = {R_PQ, cur ? R_RZ1 : R_RZ0};
+                double tot[2];
+                member_totals<2>(J, cm, kinds, tot, sh);
+                if (tid == 0) publish64(J, cm, 2 * it + 2, 0, (tot[0] != 0.0) ? tot[1] / tot[0] : 0.0);
+            }
+        }
+        if (!any) break;
+        // phase B: x += alpha p; r -= alpha q; z = invD r; (r.r, r.z) partials; the last arriver
+        // takes the checkpoint decision and publishes the next beta
+        {
+            const int srr = (it & 1) ? R_RR1 : R_RR0, srz = (it & 1) ? R_RZ1 : R_RZ0;
+            int cm = -1;
+            bool on = false;
+            double alpha = 0.0;
+            for (int t = tb0; t < tb1; t++) {
+                const int m = J.tile_mem[t];
+                if (m != cm) {
+                    if (cm >= 0 && on && arrive64(J, cm, &shv)) publish_beta(J, cm, it + 1, sh);
+                    cm = m;
+                    on = false;
+                    if (uniform_ld(&J.mdone[m], &shv) < 0) {
+                        const int st = wait64(J, m, 2 * it + 2, 0, &shd, &shv);
+                        if (st < 0) return;
+                        on = st == 1;
+                        alpha = shd;
+                    }
+                }
+                if (!on) continue;
+                const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
+                double v[2] = {0.0, 0.0};
+                for (int i = r0 + tid; i < r1; i += kThreads) {
+                    J.x[i] += alpha * pn[i];
+                    const double ri = J.r[i] - alpha * J.q[i];
+                    const double zi = J.invD[i] * ri;
+                    J.r[i] = ri; J.z[i] = zi;
+                    v[0] += ri * ri; v[1] += ri * zi;
+                }
+                const int kinds[2] = {srr, srz};
+                put_partials<2>(J, t, kinds, v, sh);
+            }
+            if (cm >= 0 && on && arrive64(J, cm, &shv)) publish_beta(J, cm, it + 1, sh);
         }
     }
 }
@@ -656,7 +732,7 @@ struct JcgWork {
     int32_t* mctl = nullptr;
     int32_t *mdone = nullptr, *mouter = nullptr, *minner = nullptr, *mret = nullptr, *mgen = nullptr;
     unsigned* mcnt = nullptr;
-    int32_t* mnblk = nullptr;
+    int32_t *mnblk = nullptr, *mnblk64 = nullptr;   // blocks holding each member's tiles (IR, FP64 grids)
     unsigned* ndone = nullptr;
 };
 
@@ -734,19 +810,24 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     A((void**)&w->mem_ab, 72 * (size_t)nmem);
     A((void**)&w->mctl, 4 * (6 * (size_t)nmem + 2));
     A((void**)&w->mnblk, 4 * (size_t)nmem);
+    A((void**)&w->mnblk64, 4 * (size_t)nmem);
     if (e != cudaSuccess) return e;
     w->mdone = w->mctl; w->mouter = w->mctl + nmem; w->minner = w->mctl + 2 * nmem; w->mret = w->mctl + 3 * nmem;
     w->mgen = w->mctl + 4 * nmem; w->mcnt = (unsigned*)(w->mctl + 5 * nmem);
     w->ndone = (unsigned*)(w->mctl + 6 * nmem);
     {
-        // blocks of the refinement grid holding tiles of each member
-        std::vector<int32_t> nb(nmem, 0);
-        for (int b = 0; b < w->gridir; b++) {
-            int last = -1;
-            for (int t = bir[b]; t < bir[b + 1]; t++)
-                if (tm[t] != last) { last = tm[t]; nb[last]++; }
-        }
-        cudaMemcpy(w->mnblk, nb.data(), 4 * (size_t)nmem, cudaMemcpyHostToDevice);
+        // blocks of each grid holding tiles of each member
+        auto count = [&](const std::vector<int32_t>& bt, int grid, int32_t* dst) {
+            std::vector<int32_t> nb(nmem, 0);
+            for (int b = 0; b < grid; b++) {
+                int last = -1;
+                for (int t = bt[b]; t < bt[b + 1]; t++)
+                    if (tm[t] != last) { last = tm[t]; nb[last]++; }
+            }
+            cudaMemcpy(dst, nb.data(), 4 * (size_t)nmem, cudaMemcpyHostToDevice);
+        };
+        count(bir, w->gridir, w->mnblk);
+        count(b64, w->grid64, w->mnblk64);
     }
     cudaMemcpy(w->tile_r0, tr0.data(), 4 * T, cudaMemcpyHostToDevice);
     cudaMemcpy(w->tile_r1, tr1.data(), 4 * T, cudaMemcpyHostToDevice);
@@ -763,7 +844,7 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
 void jcg_work_free(JcgWork* w) {
     if (!w) return;
     void* ps[] = {w->tile_r0, w->tile_r1, w->tile_mem, w->mem_t0, w->mem_t1, w->blk64, w->blkir,
-                  w->tile_part, w->mem_atol2, w->mem_ab, w->mctl, w->mnblk};
+                  w->tile_part, w->mem_atol2, w->mem_ab, w->mctl, w->mnblk, w->mnblk64};
     for (void* p : ps) cudaFree(p);
     delete w;
 }
@@ -782,7 +863,7 @@ cudaError_t jcg_launch(const JcgArgs& a, JcgWork* w, cudaStream_t st, int nsm) {
     J.tile_part = w->tile_part; J.mem_atol2 = w->mem_atol2;
     J.mdone = w->mdone; J.mouter = w->mouter; J.minner = w->minner; J.mret = w->mret; J.ndone = w->ndone;
     J.mem_ab = w->mem_ab; J.mpub = w->mem_ab + 4 * (size_t)w->nmem;
-    J.mgen = w->mgen; J.mcnt = w->mcnt; J.mnblk = w->mnblk;
+    J.mgen = w->mgen; J.mcnt = w->mcnt; J.mnblk = ir ? w->mnblk : w->mnblk64;
     J.bar = a.bar; J.err = a.err;
     J.rtol = a.rtol; J.maxiter = a.maxiter; J.check_every = a.check_every > 0 ? a.check_every : 1;
     J.inner_rtol = a.inner_rtol; J.inner_maxiter = a.inner_maxiter;
@@ -830,7 +911,8 @@ constexpr size_t kNoAllocBytes = kNaOffCtl + kNaCtlBytes;                // abou
 static __device__ __align__(256) unsigned char gs_noalloc_scratch[kNoAllocBytes];
 
 // control words at kNaOffCtl: [0] mem_t0, [1] mem_t1, [2] mdone, [3] mouter, [4] ndone,
-// [5] grid barrier word, [6] unused, [7] err
+// [5] grid barrier word, [6] unused, [7] err, [8] mgen, [9] mcnt, [10] mnblk (= grid: every
+// block holds tiles of the one member); published scalars at kNaOffAtol + 64
 
 __global__ void k_noalloc_setup(unsigned char* base, int n, const int32_t* indptr, const int32_t* indices,
                                 const double* A, int ntiles, int grid) {
@@ -848,7 +930,7 @@ __global__ void k_noalloc_setup(unsigned char* base, int n, const int32_t* indpt
         tm[t] = 0;
     }
     for (int b = gid; b <= grid; b += G) bt[b] = (int32_t)((long long)ntiles * b / grid);
-    if (gid < (int)(kNaCtlBytes / 4)) ctl[gid] = (gid == 1) ? ntiles : (gid == 2 ? -1 : 0);
+    if (gid < (int)(kNaCtlBytes / 4)) ctl[gid] = (gid == 1) ? ntiles : (gid == 2 ? -1 : (gid == 10 ? grid : 0));
     for (int i = gid; i < n; i += G) {
         double dg = 0.0;
         for (int a = indptr[i]; a < indptr[i + 1]; a++)
@@ -911,6 +993,8 @@ extern "C" gs_status gs_jcg_solve_csr_noalloc(int n, const int32_t* indptr, cons
     J.mem_t0 = ctl + 0; J.mem_t1 = ctl + 1; J.mdone = ctl + 2; J.mouter = ctl + 3;
     J.ndone = (unsigned*)(ctl + 4); J.bar = (unsigned*)(ctl + 5);
     J.err = ctl + 7;
+    J.mgen = ctl + 8; J.mcnt = (unsigned*)(ctl + 9); J.mnblk = ctl + 10;
+    J.mpub = (double*)(base + kNaOffAtol + 64);
     J.rtol = rtol; J.maxiter = maxiter; J.check_every = check_every > 0 ? check_every : 1;
     void* args[] = {&J};
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_jcg64<false>, dim3(grid), dim3(kThreads), args, 0, st);

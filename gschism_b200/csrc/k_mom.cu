@@ -1,7 +1,8 @@
 // Momentum and vertical velocity (meshdata.cu:5045-5454, 5978-6103) plus the horizontal
 // advective fluxes of transport (computeHorizAdvecFluxes, :6461-6491), fused per side: one
-// thread owns one side column, solves its vertical tridiagonal system in registers/local
-// memory and writes u2 and Qh level by level (level-major arrays, coalesced across sides).
+// thread owns one side column, solves its vertical tridiagonal system with the intermediate
+// values kept in the level-major output arrays (coalesced across sides, no local memory) and
+// writes u2 and Qh level by level.
 #include "dev_common.cuh"
 #include "kernels.h"
 
@@ -32,14 +33,33 @@ __device__ __forceinline__ double2 side_grad_eta(const Dev& d, const Phys& P, in
     return g;
 }
 
+// Horizontal advective flux through side s between levels k-1 and k (computeHorizAdvecFluxes)
+__device__ __forceinline__ double side_flux(double len, double nx, double ny, double zk, double zkm1, double2 uk,
+                                            double2 ukm1) {
+    const double area = len * (zk - zkm1);
+    const double vn1 = nx * uk.x + ny * uk.y;
+    const double vn2 = nx * ukm1.x + ny * ukm1.y;
+    return area * (0.5 * (vn1 + vn2));
+}
+
+// applyMomentumBC on a land side: free slip (islip = 0) keeps the tangential component
+__device__ __forceinline__ double2 slip(double2 u, int8_t bt, double nx, double ny) {
+    if (bt != 1) return u;
+    const double2 t = v2(-ny, nx), nn = v2(nx, ny);
+    const double vnorm = 0.0;
+    const double vtan = dot2(u, t);
+    return t * vtan - nn * vnorm;
+}
+
 __global__ void __launch_bounds__(128) k_momentum(Dev d, Phys P) {
     const int NS = d.NS, nvrt = P.nvrt;
     const double dt = P.dt, th = P.thetai;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < NS; s += gridDim.x * blockDim.x) {
         double2* u2 = d.su2;
         const double2* btu = d.btu;
+        double* Qh = d.Qh;
         if (d.sdry[s]) {
-            for (int k = 0; k < nvrt; k++) { u2[(size_t)k * NS + s] = v2(0.0, 0.0); d.Qh[(size_t)k * NS + s] = -1.0e34; }
+            for (int k = 0; k < nvrt; k++) { u2[(size_t)k * NS + s] = v2(0.0, 0.0); Qh[(size_t)k * NS + s] = -1.0e34; }
             continue;
         }
         // computeHorGradientAtSide (pressure and tidal potential gradients are zero)
@@ -52,107 +72,118 @@ __global__ void __launch_bounds__(128) k_momentum(Dev d, Phys P) {
         const double cor = d.cori[s];
         const double2 tau2 = (v2(d.tau[2 * a], d.tau[2 * a + 1]) + v2(d.tau[2 * b], d.tau[2 * b + 1])) * 0.5;
         const double cd = 0.5 * (d.drag[a] + d.drag[b]);
-        double2 ucol[kMaxLevels];
-        if (kb == nvrt - 2) {
+        const int8_t bt = d.sbt[s];
+        const double nx = d.snx[s], ny = d.sny[s], len = d.len[s];
+        const bool two_d = (kb == nvrt - 2);
+        double2 vel2d = v2(0.0, 0.0);   // 2D column: one velocity for every level
+        double2 rtop = v2(0.0, 0.0);    // 3D column: the top row's value after the forward sweep
+        if (two_d) {
             const double htot = d.zc[(size_t)(nvrt - 1) * NS + s] - d.zc[(size_t)kb * NS + s];
             const double hhat = d.hhat[s];
             const double2 un = u2[(size_t)(nvrt - 1) * NS + s];
             const double2 corT = v2(un.y, -un.x) * cor;
             const double2 inner = (corT + tau2 / htot) - (gE1 * (1 - th) + gE2 * th) * grav3;
             const double2 hat_gam = btu[(size_t)(nvrt - 1) * NS + s] + inner * dt;
-            const double2 vel = clampvel((hat_gam * hhat) / htot, P.rmaxvel);
-            for (int k = 0; k < nvrt; k++) ucol[k] = vel;
+            vel2d = clampvel((hat_gam * hhat) / htot, P.rmaxvel);
         } else {
-            double alow[kMaxLevels], cupp[kMaxLevels], bdia[kMaxLevels], gam[kMaxLevels];
-            double2 rh[kMaxLevels];
+            // assembly of row k (solveMomentumEquations, meshdata.cu:5076-5354) and the forward
+            // sweep of tridag_sch<2> (meshdata.cu:3664-3716); the sweep's values replace u2[k]
+            // (the old u2[k] stays in a register for row k+1), the eliminated super-diagonal goes
+            // to Qh[k] until the fluxes overwrite it
             const double2 grad2D = (gE2 * th + gE1 * (1.0 - th)) * grav3;
             const double dfz = 0.5 * (P.dfv0 + P.dfv0);
+            double2 ukm1 = v2(0.0, 0.0), bkm1 = v2(0.0, 0.0);
+            double2 uk = u2[(size_t)(kb + 1) * NS + s], bk = btu[(size_t)(kb + 1) * NS + s];
+            double zkm1 = d.zc[(size_t)kb * NS + s], zk = d.zc[(size_t)(kb + 1) * NS + s];
+            double bet = 0.0, cprev = 0.0;
+            double2 rprev = v2(0.0, 0.0);
             for (int k = kb + 1; k < nvrt; k++) {
-                const int kin = k - (kb + 1);
-                alow[kin] = 0.0; cupp[kin] = 0.0; bdia[kin] = 0.0;
+                const bool top = (k == nvrt - 1);
+                const double2 ukp1 = top ? v2(0.0, 0.0) : u2[(size_t)(k + 1) * NS + s];
+                const double2 bkp1 = top ? v2(0.0, 0.0) : btu[(size_t)(k + 1) * NS + s];
+                const double zkp1 = top ? 0.0 : d.zc[(size_t)(k + 1) * NS + s];
+                double alow = 0.0, cupp = 0.0, bdia = 0.0;
                 const double cff1 = 1.0;
-                const double dz_0 = d.zc[(size_t)k * NS + s] - d.zc[(size_t)(k - 1) * NS + s];
-                const double dz_1 = (k < nvrt - 1) ? d.zc[(size_t)(k + 1) * NS + s] - d.zc[(size_t)k * NS + s] : 0.0;
-                if (k < nvrt - 1) {
+                const double dz_0 = zk - zkm1;
+                const double dz_1 = !top ? zkp1 - zk : 0.0;
+                if (!top) {
                     const double tmp = dt * dfz / dz_1;
-                    cupp[kin] += cff1 * dz_1 / 6.0 - tmp;
-                    bdia[kin] += cff1 * dz_1 / 3.0 + tmp;
+                    cupp += cff1 * dz_1 / 6.0 - tmp;
+                    bdia += cff1 * dz_1 / 3.0 + tmp;
                 }
                 if (k > kb + 1) {
                     const double tmp = dt * dfz / dz_0;
-                    alow[kin] += cff1 * dz_0 / 6.0 - tmp;
-                    bdia[kin] += cff1 * dz_0 / 3.0 + tmp;
+                    alow += cff1 * dz_0 / 6.0 - tmp;
+                    bdia += cff1 * dz_0 / 3.0 + tmp;
                 } else {
-                    bdia[kin] += dt * d.chi2[s];
+                    bdia += dt * d.chi2[s];
                 }
                 double dz = 0.0;
                 dz += dz_1;
                 if (k > kb + 1) dz += dz_0;
                 double2 r = grad2D * (-(0.5 * dz) * dt);
-                const double2 uk = u2[(size_t)k * NS + s];
-                const double2 bk = btu[(size_t)k * NS + s];
-                if (k < nvrt - 1) {
-                    const double2 uu = uk * 2.0 + u2[(size_t)(k + 1) * NS + s];
+                if (!top) {
+                    const double2 uu = uk * 2.0 + ukp1;
                     const double2 ct = v2(uu.y, -uu.x) * cor;
-                    const double2 in = (bk * 2.0 + btu[(size_t)(k + 1) * NS + s]) + ct * dt;
+                    const double2 in = (bk * 2.0 + bkp1) + ct * dt;
                     r = r + in * (dz_1 / 6.0);
                 } else {
                     r = r + tau2 * dt;
                 }
                 if (k > kb + 1) {
-                    const double2 uu = uk * 2.0 + u2[(size_t)(k - 1) * NS + s];
+                    const double2 uu = uk * 2.0 + ukm1;
                     const double2 ct = v2(uu.y, -uu.x) * cor;
-                    const double2 in = (bk * 2.0 + btu[(size_t)(k - 1) * NS + s]) + ct * dt;
+                    const double2 in = (bk * 2.0 + bkm1) + ct * dt;
                     r = r + in * (dz_0 / 6.0);
                 }
-                rh[kin] = r;
-            }
-            // tridag_sch<2>, meshdata.cu:3664-3716
-            const int n = nvrt - kb - 1;
-            double bet = bdia[0];
-            rh[0] = v2(rh[0].x / bet, rh[0].y / bet);
-            for (int j = 1; j < n; j++) {
-                gam[j] = cupp[j - 1] / bet;
-                bet = bdia[j] - alow[j] * gam[j];
-                rh[j] = v2((rh[j].x - alow[j] * rh[j - 1].x) / bet, (rh[j].y - alow[j] * rh[j - 1].y) / bet);
-            }
-            for (int j = n - 2; j >= 0; j--)
-                rh[j] = v2(rh[j].x - gam[j + 1] * rh[j + 1].x, rh[j].y - gam[j + 1] * rh[j + 1].y);
-            for (int k = kb + 1; k < nvrt; k++) ucol[k] = clampvel(rh[k - kb - 1], P.rmaxvel);
-        }
-        if (cd == 0.0) ucol[kb] = ucol[kb + 1];
-        else if (kb != nvrt - 2) ucol[kb] = v2(0.0, 0.0);
-        for (int k = 0; k < kb; k++) ucol[k] = v2(0.0, 0.0);
-        // applyMomentumBC: free slip on land sides (islip = 0)
-        const int8_t bt = d.sbt[s];
-        const double nx = d.snx[s], ny = d.sny[s];
-        if (bt == 1) {
-            const double2 t = v2(-ny, nx), nn = v2(nx, ny);
-            for (int k = kb; k < nvrt; k++) {
-                const double vnorm = 0.0;
-                const double vtan = dot2(ucol[k], t);
-                ucol[k] = t * vtan - nn * vnorm;
-            }
-        }
-        // store u2 and the horizontal advective fluxes Qh (land sides carry zero flux)
-        const double len = d.len[s];
-        double zprev = d.zc[(size_t)kb * NS + s];
-        for (int k = 0; k < nvrt; k++) {
-            u2[(size_t)k * NS + s] = ucol[k];
-            double qh = -1.0e34;
-            if (k > kb) {
-                const double zk = d.zc[(size_t)k * NS + s];
-                if (bt == 1) qh = 0.0;
-                else {
-                    const double area = len * (zk - zprev);
-                    const double vn1 = nx * ucol[k].x + ny * ucol[k].y;
-                    const double vn2 = nx * ucol[k - 1].x + ny * ucol[k - 1].y;
-                    qh = area * (0.5 * (vn1 + vn2));
+                if (k == kb + 1) {
+                    bet = bdia;
+                    r = v2(r.x / bet, r.y / bet);
+                } else {
+                    const double gam = cprev / bet;
+                    bet = bdia - alow * gam;
+                    r = v2((r.x - alow * rprev.x) / bet, (r.y - alow * rprev.y) / bet);
+                    Qh[(size_t)k * NS + s] = gam;
                 }
-                zprev = zk;
+                u2[(size_t)k * NS + s] = r;
+                rprev = r;
+                cprev = cupp;
+                ukm1 = uk; uk = ukp1; bkm1 = bk; bk = bkp1; zkm1 = zk; zk = zkp1;
             }
-            d.Qh[(size_t)k * NS + s] = qh;
+            rtop = rprev;
         }
+        // top-down: back substitution (3D), clamp, the bottom level's value, free slip on land
+        // sides, and the stores of u2 and of the fluxes Qh (land sides carry zero flux)
+        double2 r = rtop, uabove = v2(0.0, 0.0);
+        double zabove = 0.0;
+        for (int k = nvrt - 1; k >= kb; k--) {
+            double2 u;
+            if (k > kb) {
+                if (two_d) {
+                    u = vel2d;
+                } else {
+                    if (k < nvrt - 1) {
+                        const double gam = Qh[(size_t)(k + 1) * NS + s];
+                        const double2 x = u2[(size_t)k * NS + s];
+                        r = v2(x.x - gam * r.x, x.y - gam * r.y);
+                    }
+                    u = clampvel(r, P.rmaxvel);
+                }
+            } else {
+                // ucol[kb]: the level above when there is no bottom drag, else 0 (3D) / the 2D value
+                if (cd == 0.0) u = two_d ? vel2d : clampvel(r, P.rmaxvel);
+                else u = two_d ? vel2d : v2(0.0, 0.0);
+            }
+            u = slip(u, bt, nx, ny);
+            u2[(size_t)k * NS + s] = u;
+            const double zk = d.zc[(size_t)k * NS + s];
+            if (k < nvrt - 1)
+                Qh[(size_t)(k + 1) * NS + s] = (bt == 1) ? 0.0 : side_flux(len, nx, ny, zabove, zk, uabove, u);
+            uabove = u;
+            zabove = zk;
+        }
+        Qh[(size_t)kb * NS + s] = -1.0e34;
+        for (int k = 0; k < kb; k++) { u2[(size_t)k * NS + s] = v2(0.0, 0.0); Qh[(size_t)k * NS + s] = -1.0e34; }
     }
 }
 

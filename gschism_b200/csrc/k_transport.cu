@@ -5,7 +5,16 @@
 // remaining time and sub-step on the device (the reference reads minTransportDt back to the
 // host once per sub-step).  The minimum admissible sub-step of a member is reduced with an
 // integer atomicMin on the bit pattern of non-negative doubles, which is order-independent.
-// The implicit vertical advection of an element is fused into its member's last sub-step.
+//
+// The reference copies every element's tracers into a snapshot before each sub-step and reads
+// the neighbours from it.  Here the two tracer arrays alternate instead: sub-step s reads one
+// (etr for even s, prev for odd s) and writes the other, so no copy is made; after a member's
+// last sub-step its result sits in prev when it took an odd number of sub-steps.  The implicit
+// vertical advection runs after every member has finished sub-cycling, reads the result from
+// where it sits and writes etr; its Thomas sweep recomputes each row's coefficients and keeps the
+// forward-sweep values in etr and the eliminated super-diagonal in prev (both level-major, so a
+// warp's accesses are coalesced), instead of per-thread arrays in local memory.  The tracer count
+// is a template parameter, so per-tracer values stay in registers.
 #include "dev_common.cuh"
 #include "kernels.h"
 
@@ -26,38 +35,93 @@ __device__ __forceinline__ double evol(const Dev& d, int e, int k) {
     return d.area[e] * (d.ez[(size_t)(k + 1) * d.NE + e] - d.ez[(size_t)k * d.NE + e]);
 }
 
-__device__ void vertical_upwind(const Dev& d, const Phys& P, int e, double dt) {
-    // verticalAdvectionUpdate, meshdata.cu:6611-6665 (upwind: phi = 0)
-    const int NE = d.NE, nvrt = P.nvrt, ntr = P.ntr;
-    const int kb = d.kbe[e];
-    const int nEq = nvrt - (kb + 1);
-    double alow[kMaxLevels], bdia[kMaxLevels], cupp[kMaxLevels], gam[kMaxLevels], u[kMaxLevels];
-    for (int k = kb + 1; k < nvrt; k++) {
-        const int kin = k - (kb + 1);
-        alow[kin] = 0.0; cupp[kin] = 0.0; bdia[kin] = 0.0;
-        const double dbv = dt / evol(d, e, k - 1);
-        bdia[kin] += 1.0;
-        const double qk = d.Qv[(size_t)k * NE + e], qm = d.Qv[(size_t)(k - 1) * NE + e];
-        if (k != nvrt - 1 && qk < 0.0) { const double tmp = dbv * fabs(qk); cupp[kin] -= tmp; bdia[kin] += tmp; }
-        if (k - 1 != kb && qm > 0.0) { const double tmp = dbv * fabs(qm); alow[kin] -= tmp; bdia[kin] += tmp; }
+// The three sides of element e as the horizontal update needs them (loaded once per element).
+struct ElemSides {
+    int s[3], kbs[3], nb[3];
+    double sg[3];
+    bool nbwet[3];
+    int8_t bt[3];
+};
+
+__device__ __forceinline__ ElemSides elem_sides(const Dev& d, int e) {
+    ElemSides q;
+    const int NE = d.NE, NS = d.NS;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int s = d.es[j * NE + e];
+        q.s[j] = s;
+        q.kbs[j] = d.kbs[s];
+        const int e0 = d.se[s], e1 = d.se[NS + s];
+        const int nb = (e0 == e) ? e1 : e0;
+        q.nb[j] = nb;
+        q.nbwet[j] = nb >= 0 && !d.edry[nb];
+        q.sg[j] = (double)d.ssgn[j * NE + e];
+        q.bt[j] = d.sbt[s];
     }
-    for (int t = 0; t < ntr; t++) {
-        double* tr = d.etr + (size_t)t * nvrt * NE;
-        double bet = bdia[0];
-        u[0] = (tr[(size_t)(kb + 1) * NE + e] * 1.0) / bet;
-        for (int j = 1; j < nEq; j++) {
-            gam[j] = cupp[j - 1] / bet;
-            bet = bdia[j] - alow[j] * gam[j];
-            u[j] = (tr[(size_t)(kb + 1 + j) * NE + e] * 1.0 - alow[j] * u[j - 1]) / bet;
-        }
-        for (int j = nEq - 2; j >= 0; j--) u[j] = u[j] - gam[j + 1] * u[j + 1];
-        for (int k = kb + 1; k < nvrt; k++) tr[(size_t)k * NE + e] = u[k - (kb + 1)];
-        for (int k = 0; k <= kb; k++) tr[(size_t)k * NE + e] = u[0];
-    }
+    return q;
 }
 
+// verticalAdvectionUpdate, meshdata.cu:6611-6665 (upwind: phi = 0) for the NTR tracers of
+// element e: reads the column from src, writes it to dst (src may equal dst), uses scr (one
+// level-major slice) for the eliminated super-diagonal.  Same arithmetic as the reference's
+// tridag_sch<1> (meshdata.cu:3664-3716) row by row.
+template <int NTR>
+__device__ void vertical_upwind(const Dev& d, const Phys& P, int e, double dt, const double* src, double* dst,
+                                double* scr) {
+    const int NE = d.NE, nvrt = P.nvrt;
+    const size_t trs = (size_t)nvrt * NE;
+    const int kb = d.kbe[e];
+    const int k0 = kb + 1;
+    if (k0 >= nvrt) return;          // a wet element has at least one layer
+    double bet = 0.0, cprev = 0.0;
+    double up[NTR];
+    for (int k = k0; k < nvrt; k++) {
+        double alow = 0.0, cupp = 0.0, bdia = 0.0;
+        const double dbv = dt / evol(d, e, k - 1);
+        bdia += 1.0;
+        const double qk = d.Qv[(size_t)k * NE + e], qm = d.Qv[(size_t)(k - 1) * NE + e];
+        if (k != nvrt - 1 && qk < 0.0) { const double tmp = dbv * fabs(qk); cupp -= tmp; bdia += tmp; }
+        if (k - 1 != kb && qm > 0.0) { const double tmp = dbv * fabs(qm); alow -= tmp; bdia += tmp; }
+        const size_t ix = (size_t)k * NE + e;
+        if (k == k0) {
+            bet = bdia;
+#pragma unroll
+            for (int t = 0; t < NTR; t++) {
+                up[t] = (src[t * trs + ix] * 1.0) / bet;
+                dst[t * trs + ix] = up[t];
+            }
+        } else {
+            const double gam = cprev / bet;
+            bet = bdia - alow * gam;
+#pragma unroll
+            for (int t = 0; t < NTR; t++) {
+                up[t] = (src[t * trs + ix] * 1.0 - alow * up[t]) / bet;
+                dst[t * trs + ix] = up[t];
+            }
+            scr[ix] = gam;           // after the reads: scr may be src's first tracer slice
+        }
+        cprev = cupp;
+    }
+    // back substitution: u_j -= gam_{j+1} u_{j+1}; up holds the top level's value
+    for (int k = nvrt - 2; k >= k0; k--) {
+        const double gam = scr[(size_t)(k + 1) * NE + e];
+        const size_t ix = (size_t)k * NE + e;
+#pragma unroll
+        for (int t = 0; t < NTR; t++) {
+            up[t] = dst[t * trs + ix] - gam * up[t];
+            dst[t * trs + ix] = up[t];
+        }
+    }
+    // levels at and below the bed take the bottom prism's value
+    for (int k = 0; k <= kb; k++)
+#pragma unroll
+        for (int t = 0; t < NTR; t++) dst[t * trs + (size_t)k * NE + e] = up[t];
+}
+
+template <int NTR>
 __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
-    const int NE = d.NE, NS = d.NS, nvrt = P.nvrt, ntr = P.ntr, nmem = d.nmem;
+    const int NE = d.NE, NS = d.NS, nvrt = P.nvrt, nmem = d.nmem;
+    const size_t trs = (size_t)nvrt * NE;
     const int G = gridDim.x * blockDim.x;
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned long long seed = (unsigned long long)__double_as_longlong(1e34);
@@ -71,28 +135,24 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
     for (int sub = 0; sub < T.maxsub; sub++) {
         if (*((volatile unsigned*)T.active) == 0u) break;
         const int par = sub & 1, nxt = par ^ 1;
-        // horizontalAdvectionPrepare (meshdata.cu:6493-6559): snapshot, inflow, max sub-step
+        const double* src = par ? d.prev : d.etr;     // the sub-step's snapshot
+        double* dst = par ? d.etr : d.prev;
+        // horizontalAdvectionPrepare (meshdata.cu:6493-6559): inflow and max sub-step per element
         for (int e = gid; e < NE; e += G) {
             const int m = d.elem_member[e];
             if (!(((volatile double*)T.rem)[par * nmem + m] > 0.0) || d.edry[e]) continue;
             const int kb = d.kbe[e];
-            for (int t = 0; t < ntr; t++)
-                for (int k = 0; k < nvrt; k++) {
-                    const size_t ix = ((size_t)t * nvrt + k) * NE + e;
-                    d.prev[ix] = d.etr[ix];
-                }
+            const ElemSides q = elem_sides(d, e);
             double md = kHuge;
             for (int k = kb + 1; k < nvrt; k++) {
                 double in = 0.0;
+#pragma unroll
                 for (int j = 0; j < 3; j++) {
-                    const int s = d.es[j * NE + e];
-                    if (k <= d.kbs[s]) continue;
-                    const int e0 = d.se[s], e1 = d.se[NS + s];
-                    const int nb = (e0 == e) ? e1 : e0;
-                    if (nb < 0 || d.edry[nb]) continue;
-                    const double fq = d.Qh[(size_t)k * NS + s];
-                    const bool influx = ((double)d.ssgn[j * NE + e] * fq) < 0.0;
-                    if (d.sbt[s] == 1 || !influx) continue;
+                    if (k <= q.kbs[j]) continue;
+                    if (!q.nbwet[j]) continue;
+                    const double fq = d.Qh[(size_t)k * NS + q.s[j]];
+                    const bool influx = (q.sg[j] * fq) < 0.0;
+                    if (q.bt[j] == 1 || !influx) continue;
                     in += fabs(fq);
                 }
                 const double pd = (in == 0.0) ? kHuge : evol(d, e, k - 1) / in * (1.0 - 1.0e-6);
@@ -118,51 +178,65 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
             }
             if (d.edry[e]) continue;
             const int kb = d.kbe[e];
+            const ElemSides q = elem_sides(d, e);
             for (int k = kb + 1; k < nvrt; k++) {
+                const size_t ix = (size_t)k * NE + e;
                 const double vol = evol(d, e, k - 1);
                 const double dbv = dtb / vol;
-                double adv[kMaxTracers];
-                for (int t = 0; t < ntr; t++) adv[t] = d.prev[((size_t)t * nvrt + k) * NE + e];
+                double own[NTR], adv[NTR];
+#pragma unroll
+                for (int t = 0; t < NTR; t++) { own[t] = src[t * trs + ix]; adv[t] = own[t]; }
+#pragma unroll
                 for (int j = 0; j < 3; j++) {
-                    const int s = d.es[j * NE + e];
-                    if (k <= d.kbs[s]) continue;
-                    const double fq = d.Qh[(size_t)k * NS + s];
-                    const double sQ = (double)d.ssgn[j * NE + e] * fq;
+                    if (k <= q.kbs[j]) continue;
+                    const double fq = d.Qh[(size_t)k * NS + q.s[j]];
+                    const double sQ = q.sg[j] * fq;
                     if (sQ >= 0.0) continue;
-                    const int e0 = d.se[s], e1 = d.se[NS + s];
-                    const int nb = (e0 == e) ? e1 : e0;
                     const double coef = dbv * fabs(fq);
-                    if (nb >= 0 && !d.edry[nb]) {
-                        for (int t = 0; t < ntr; t++)
-                            adv[t] += coef * (d.prev[((size_t)t * nvrt + k) * NE + nb] - d.prev[((size_t)t * nvrt + k) * NE + e]);
-                    } else if (d.sbt[s] == 2) {
-                        for (int t = 0; t < ntr; t++) {
+                    if (q.nbwet[j]) {
+                        const size_t nx = (size_t)k * NE + q.nb[j];
+#pragma unroll
+                        for (int t = 0; t < NTR; t++) adv[t] += coef * (src[t * trs + nx] - own[t]);
+                    } else if (q.bt[j] == 2) {
+#pragma unroll
+                        for (int t = 0; t < NTR; t++) {
                             const double cout = adv[t];
-                            adv[t] += coef * (cout - d.prev[((size_t)t * nvrt + k) * NE + e]);
+                            adv[t] += coef * (cout - own[t]);
                         }
                     }
                 }
-                for (int t = 0; t < ntr; t++) d.etr[((size_t)t * nvrt + k) * NE + e] = adv[t];
+#pragma unroll
+                for (int t = 0; t < NTR; t++) dst[t * trs + ix] = adv[t];
             }
-            for (int t = 0; t < ntr; t++) {
-                const double v = d.etr[((size_t)t * nvrt + kb + 1) * NE + e];
-                for (int k = 0; k <= kb; k++) d.etr[((size_t)t * nvrt + k) * NE + e] = v;
+#pragma unroll
+            for (int t = 0; t < NTR; t++) {
+                const double v = dst[t * trs + (size_t)(kb + 1) * NE + e];
+                for (int k = 0; k <= kb; k++) dst[t * trs + (size_t)k * NE + e] = v;
             }
-            if (last) vertical_upwind(d, P, e, T.dt);
         }
         if (!grid_sync(d.bar, d.err)) return;
     }
+    // verticalAdvectionUpdate for every wet element, once its member has finished sub-cycling:
+    // after n sub-steps the horizontal result is in prev when n is odd, in etr when it is even
+    for (int e = gid; e < NE; e += G) {
+        if (d.edry[e]) continue;
+        const int m = d.elem_member[e];
+        const double* res = (T.nsub[m] & 1) ? d.prev : d.etr;
+        vertical_upwind<NTR>(d, P, e, T.dt, res, d.etr, d.prev);
+    }
 }
 
+template <int NTR>
 __global__ void k_nodal_tracer(Dev d, Phys P) {
     // nodalTracerUpdate, meshdata.cu:6739-6774 (node-centred gather, no atomics)
-    const int NP = d.NP, NE = d.NE, nvrt = P.nvrt, ntr = P.ntr, ivrt = nvrt - 1;
+    const int NP = d.NP, NE = d.NE, nvrt = P.nvrt, ivrt = nvrt - 1;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NP; i += gridDim.x * blockDim.x) {
         if (d.ndry[i]) continue;
         const int q0 = d.nne_s[i], q1 = d.nne_s[i + 1];
         for (int k = 0; k < nvrt; k++) {
-            double sum[kMaxTracers];
-            for (int t = 0; t < ntr; t++) sum[t] = 0.0;
+            double sum[NTR];
+#pragma unroll
+            for (int t = 0; t < NTR; t++) sum[t] = 0.0;
             double sumA = 0.0;
             for (int q = q0; q < q1; q++) {
                 const int e = d.nne[q];
@@ -179,7 +253,8 @@ __global__ void k_nodal_tracer(Dev d, Phys P) {
                     zrat = (zp - zc) / (zp - zm);
                 }
                 const double A = d.area[e];
-                for (int t = 0; t < ntr; t++) {
+#pragma unroll
+                for (int t = 0; t < NTR; t++) {
                     const double* tr = d.etr + (size_t)t * nvrt * NE;
                     sum[t] += A * ((1.0 - zrat) * tr[(size_t)kHi * NE + e] + zrat * tr[(size_t)kLo * NE + e]);
                 }
@@ -187,17 +262,16 @@ __global__ void k_nodal_tracer(Dev d, Phys P) {
             }
             if (sumA == 0.0) continue;
             const double inv = 1.0 / sumA;
-            for (int t = 0; t < ntr; t++) d.tr[((size_t)t * nvrt + k) * NP + i] = inv * sum[t];
+#pragma unroll
+            for (int t = 0; t < NTR; t++) d.tr[((size_t)t * nvrt + k) * NP + i] = inv * sum[t];
         }
     }
 }
 
-cudaError_t launch_transport(const Dev& d, const Phys& P, double dt, cudaStream_t st, int nsm) {
-    TrArgs T;
-    T.rem = d.mem_rem; T.mindt = d.mem_mindt; T.nsub = d.mem_nsub; T.active = (unsigned*)(d.mem_mindt + 2 * d.nmem);
-    T.dt = dt; T.maxsub = 100000;
+template <int NTR>
+static cudaError_t launch_ntr(const Dev& d, const Phys& P, TrArgs& T, cudaStream_t st, int nsm) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_transport, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_transport<NTR>, 256, 0);
     if (per_sm < 1) per_sm = 1;
     if (per_sm > 4) per_sm = 4;
     int grid = std::min(nsm * per_sm, (d.NE + 255) / 256);
@@ -205,10 +279,28 @@ cudaError_t launch_transport(const Dev& d, const Phys& P, double dt, cudaStream_
     Dev dd = d;
     Phys pp = P;
     void* args[] = {&dd, &pp, &T};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_transport, dim3(grid), dim3(256), args, 0, st);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_transport<NTR>, dim3(grid), dim3(256), args, 0, st);
     if (e != cudaSuccess) return e;
-    k_nodal_tracer<<<grid_for(d.NP, 128, nsm * 16), 128, 0, st>>>(d, P);
+    k_nodal_tracer<NTR><<<grid_for(d.NP, 128, nsm * 16), 128, 0, st>>>(d, P);
     return cudaGetLastError();
+}
+
+cudaError_t launch_transport(const Dev& d, const Phys& P, double dt, cudaStream_t st, int nsm) {
+    if (P.ntr <= 0) return cudaSuccess;
+    TrArgs T;
+    T.rem = d.mem_rem; T.mindt = d.mem_mindt; T.nsub = d.mem_nsub; T.active = (unsigned*)(d.mem_mindt + 2 * d.nmem);
+    T.dt = dt; T.maxsub = 100000;
+    static_assert(kMaxTracers == 8, "one instantiation per tracer count");
+    switch (P.ntr) {
+    case 1: return launch_ntr<1>(d, P, T, st, nsm);
+    case 2: return launch_ntr<2>(d, P, T, st, nsm);
+    case 3: return launch_ntr<3>(d, P, T, st, nsm);
+    case 4: return launch_ntr<4>(d, P, T, st, nsm);
+    case 5: return launch_ntr<5>(d, P, T, st, nsm);
+    case 6: return launch_ntr<6>(d, P, T, st, nsm);
+    case 7: return launch_ntr<7>(d, P, T, st, nsm);
+    default: return launch_ntr<8>(d, P, T, st, nsm);
+    }
 }
 
 }  // namespace gs

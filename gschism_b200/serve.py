@@ -28,6 +28,7 @@ import concurrent.futures as cf
 import dataclasses
 import json
 import math
+import sys
 import time
 from typing import Any, Callable, Dict, List, Optional, Sequence
 
@@ -115,7 +116,8 @@ class Server:
 
     def __init__(self, engine, budget_bytes: Optional[int] = None, max_members: int = 64,
                  steps_per_turn: int = 8, background_build: bool = True,
-                 clock: Callable[[], float] = time.perf_counter, sleep: Callable[[float], None] = time.sleep):
+                 clock: Callable[[], float] = time.perf_counter, sleep: Callable[[float], None] = time.sleep,
+                 on_finish: Optional[Callable[[Request], None]] = None):
         self.engine = engine
         self.budget = int(budget_bytes if budget_bytes is not None else 0.9 * engine.free_bytes())
         self.max_members = max_members
@@ -125,6 +127,7 @@ class Server:
         self.used = 0
         self.peak_used = 0
         self.log: List[tuple] = []
+        self.on_finish = on_finish
 
     def _admit(self, queue: List[Request], now: float, cid: int) -> Optional[_Cohort]:
         """Longest FIFO prefix of same-horizon requests that fits in the free budget."""
@@ -210,6 +213,8 @@ class Server:
                     for r, x in zip(c.reqs, res):
                         r.result = x
                         r.finished = t
+                        if self.on_finish is not None:
+                            self.on_finish(r)
                     self.engine.close(c.handle)
                     active.remove(c)
                     self.used -= c.nbytes
@@ -264,8 +269,15 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     reqs = poisson_requests(a.requests, a.rate, a.seed, hours=a.hours, nmin=a.nmin, nmax=a.nmax)
     eng = ModelEngine(precision=a.precision)
+
+    def progress(r: Request) -> None:
+        # one line per finished forecast, so a run cut short still reports what it did
+        print(json.dumps({"rid": r.rid, "nodes": int(r.case.n_nodes), "arrival_s": round(r.arrival, 3),
+                          "started_s": round(r.started, 3), "ttf_s": round(r.time_to_forecast, 3)}),
+              file=sys.stderr, flush=True)
+
     srv = Server(eng, budget_bytes=None if a.budget_gb is None else int(a.budget_gb * 1e9),
-                 steps_per_turn=a.steps_per_turn)
+                 steps_per_turn=a.steps_per_turn, on_finish=progress)
     t0 = time.perf_counter()
     srv.run(reqs)
     out = summary(reqs, time.perf_counter() - t0)

@@ -177,3 +177,25 @@ def test_graph_step_equals_phase_by_phase(native):
         by_phase(b, it)
     for f in ("ETA2", "SIDE_U2", "ELEM_TR", "NODE_TAU"):
         assert np.array_equal(a.get(0, f), b.get(0, f)), f
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_ir"])
+def test_member_at_rest_beside_a_forced_one(native, precision):
+    """A member without forcing (zero right-hand side: retired before the first iteration) in the
+    same batch as a forced member: the solve ends, the resting member stays at rest and the forced
+    one gets the same bits as alone."""
+    from gschism_b200.model import Model
+    rest = cases.channel(seed=51, nx=30, ny=16)
+    rest.emo = [np.zeros_like(a) for a in rest.emo]
+    rest.tau = np.zeros_like(rest.tau)
+    forced = cases.channel(seed=52, nx=40, ny=21)
+    mix = Model([rest, forced], precision=precision)
+    mix.step(3)
+    mix.sync()
+    assert mix.stats(0)["jcg_iters"] == 0
+    assert mix.stats(0)["error_flags"] == 0
+    assert np.all(mix.get(0, "ETA2") == 0.0)
+    alone = Model([forced], precision=precision)
+    alone.step(3)
+    assert np.array_equal(mix.get(1, "ETA2"), alone.get(0, "ETA2"))
+    assert mix.stats(1)["jcg_iters"] == alone.stats(0)["jcg_iters"]
