@@ -47,6 +47,7 @@ def _args():
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble comparison")
+    ap.add_argument("--no-serve", action="store_true", help="skip the forecast-serving run")
     return ap.parse_args()
 
 
@@ -221,6 +222,7 @@ def run_ours(a):
         return
     # the batched-ensemble comparison is a one-GPU measurement (rank 0 of a one-rank run)
     ens = run_ensemble(a, stream, local) if (ws == 1 and not a.no_ensemble) else None
+    srv = run_serving(local) if (ws == 1 and not a.no_serve) else None
     r = res["fp32_ir"]
     # roofline of the dominant kernel (JCG): algorithmic bytes / average launch time
     nnz = r["nnz"]
@@ -253,6 +255,8 @@ def run_ours(a):
                         "jcg_ms_avg": statistics.mean(f["jcg_ms"])}
     if ens is not None:
         line["ensemble"] = ens
+    if srv is not None:
+        line["serving"] = srv
     if not a.no_cpu:
         line["cpu_baseline"] = cpu_sample(a)
     print(json.dumps(line))
@@ -306,6 +310,25 @@ def run_ensemble(a, stream, local):
     out["fp64_single_instance"] = {"value": nodes * nvrt / (tot / 1e3), "ms_per_step": tot,
                                    "note": "members stepped one at a time, sum of their device times"}
     out["speedup_fp32_ir_batched_vs_fp64_single"] = tot / out["fp32_ir_batched"]["ms_per_step"]
+    return out
+
+
+def run_serving(local, n=8, rate=2.0, hours=6.0, seed=1):
+    """Forecast serving (gschism_b200/serve.py): n storm-surge requests (10k-2M nodes, 20 levels,
+    tide + vortex) arriving as a Poisson process of `rate` per second, continuous batching on this
+    GPU; time-to-forecast = arrival to results on the host.  The horizon is `hours` instead of the
+    scenario's 48 h, to keep this run to about a minute of GPU time."""
+    from gschism_b200.serve import ModelEngine, Server, poisson_requests, summary
+    reqs = poisson_requests(n, rate, seed, hours=hours)
+    srv = Server(ModelEngine(precision="fp32_ir", device=local))
+    t0 = time.perf_counter()
+    srv.run(reqs)
+    out = summary(reqs, time.perf_counter() - t0)
+    builds = [e[3] for e in srv.log if e[0] == "build"]
+    out.update({"workload": f"{n} storm-surge requests, Poisson arrivals {rate}/s, 10k-2M nodes, 20 levels, "
+                            f"{hours:g} h horizon at dt=150 s (the full scenario's horizon is 48 h)",
+                "nodes": [int(r.case.n_nodes) for r in reqs], "ttf_s": [round(r.time_to_forecast, 3) for r in reqs],
+                "build_s_total": round(sum(builds), 2)})
     return out
 
 

@@ -22,7 +22,7 @@ STATUS_NAMES = {0: "GS_OK", 1: "GS_ERR_ARG", 2: "GS_ERR_CUDA", 3: "GS_ERR_OOM", 
 PHASE = dict(BEGIN=0, BTRACK=1, PREPARE=2, ASSEMBLE=3, SOLVE=4, UPDATE_ELEV=5, MOMENTUM=6, VVEL=7,
              TRANSPORT=8, LEVELS=9, NODAL_VEL=10)
 
-EXPORTS = ["gs_grid_build", "gs_ctx_create", "gs_member_add", "gs_ctx_finalize", "gs_ctx_destroy",
+EXPORTS = ["gs_grid_build", "gs_ctx_create", "gs_member_add", "gs_ctx_prepare", "gs_ctx_finalize", "gs_ctx_destroy",
            "gs_last_error", "gs_sync", "gs_set_stream", "gs_step", "gs_phase", "gs_state_get", "gs_state_put", "gs_set_tau",
            "gs_get_stats", "gs_member_sizes", "gs_jcg_create", "gs_jcg_buffers", "gs_jcg_solve_csr",
            "gs_jcg_check", "gs_jcg_destroy", "gs_jcg_last_error", "gs_jcg_solve_csr_noalloc",
@@ -81,6 +81,7 @@ def load(build_if_missing: bool = False):
     L.gs_grid_build.argtypes = [I, I, PI, PI, PI, PI, PI, PI, PI, PI, PI, PI, PI, PI]
     L.gs_ctx_create.argtypes = [ctypes.POINTER(GsConfig), ctypes.POINTER(c_void_p)]
     L.gs_member_add.argtypes = [c_void_p, ctypes.POINTER(GsMemberDesc), ctypes.POINTER(c_int)]
+    L.gs_ctx_prepare.argtypes = [c_void_p]
     L.gs_ctx_finalize.argtypes = [c_void_p]
     L.gs_ctx_destroy.argtypes = [c_void_p]
     L.gs_last_error.argtypes = [c_void_p]

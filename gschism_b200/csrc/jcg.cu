@@ -512,10 +512,11 @@ __device__ __forceinline__ void member_arrive(const JcgView& J, int m, int it, i
     const bool done = checkpoint(J, it, J.inner_maxiter) && tot[2] <= J.mem_atol2[nmem + m];
     if (done || nit == J.inner_maxiter) {
         // the sweep ends after iteration it: keep its (alpha, gamma) and recursive r.r for the
-        // next sweep
+        // next sweep; a sweep stopped by the iteration cap leaves r.r = 0, so the next sweep
+        // restarts the recurrence instead of continuing a stalled one
         J.mem_ab[(size_t)6 * nmem + m] = J.mem_ab[(size_t)cp * nmem + m];
         J.mem_ab[(size_t)7 * nmem + m] = J.mem_ab[(size_t)(2 + cp) * nmem + m];
-        J.mem_ab[(size_t)8 * nmem + m] = tot[2];
+        J.mem_ab[(size_t)8 * nmem + m] = done ? tot[2] : 0.0;
     }
     if (done) {
         J.mret[m] = nit;
@@ -608,6 +609,10 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
                     continue;
                 }
                 if (owner) {
+                    // a sweep that did not halve the FP64 residual restarts the next one's
+                    // recurrence (the continued search directions have gone stale)
+                    if (outer > 0 && tot[0] > 0.25 * J.mem_atol2[nmem + m] / (J.inner_rtol * J.inner_rtol))
+                        J.mem_ab[(size_t)8 * nmem + m] = 0.0;
                     J.mem_atol2[nmem + m] = J.inner_rtol * J.inner_rtol * tot[0];
                     J.mouter[m] = outer + 1;
                     J.mret[m] = -1;
@@ -654,9 +659,10 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
                             // previous sweep's last (alpha, gamma) -- residual replacement every
                             // inner_rtol reduction, which keeps the FP32 recursion accurate when
                             // inner_rtol >= 1e-2 -- unless the replaced residual is more than 4x the
-                            // recursive one it replaces (r.r more than 16x).  Tighter inner
-                            // tolerances, or such a jump, restart the recurrence (beta = 0): plain
-                            // restarted refinement.
+                            // recursive one it replaces (r.r more than 16x), the previous sweep hit
+                            // the iteration cap, or it did not halve the FP64 residual.  Tighter
+                            // inner tolerances, or any of these, restart the recurrence (beta = 0):
+                            // plain restarted refinement.
                             const bool reliable = J.inner_rtol >= 1e-2;
                             const double ac = (outer > 0) ? J.mem_ab[(size_t)6 * nmem + m] : 0.0;
                             const double gc = (outer > 0) ? J.mem_ab[(size_t)7 * nmem + m] : 0.0;
@@ -772,7 +778,8 @@ static int coop_blocks(const void* fn, int nsm) {
     return nsm * per_sm;
 }
 
-cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std::vector<int>& rows, bool sell) {
+cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std::vector<int>& rows, bool sell,
+                           cudaStream_t st) {
     w = new JcgWork();
     const int nmem = (int)rows.size();
     std::vector<int32_t> tr0, tr1, tm, mt0(nmem), mt1(nmem);
@@ -824,20 +831,23 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
                 for (int t = bt[b]; t < bt[b + 1]; t++)
                     if (tm[t] != last) { last = tm[t]; nb[last]++; }
             }
-            cudaMemcpy(dst, nb.data(), 4 * (size_t)nmem, cudaMemcpyHostToDevice);
+            cudaMemcpyAsync(dst, nb.data(), 4 * (size_t)nmem, cudaMemcpyHostToDevice, st);
         };
         count(bir, w->gridir, w->mnblk);
         count(b64, w->grid64, w->mnblk64);
     }
-    cudaMemcpy(w->tile_r0, tr0.data(), 4 * T, cudaMemcpyHostToDevice);
-    cudaMemcpy(w->tile_r1, tr1.data(), 4 * T, cudaMemcpyHostToDevice);
-    cudaMemcpy(w->tile_mem, tm.data(), 4 * T, cudaMemcpyHostToDevice);
-    cudaMemcpy(w->mem_t0, mt0.data(), 4 * nmem, cudaMemcpyHostToDevice);
-    cudaMemcpy(w->mem_t1, mt1.data(), 4 * nmem, cudaMemcpyHostToDevice);
-    cudaMemcpy(w->blk64, b64.data(), 4 * b64.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(w->blkir, bir.data(), 4 * bir.size(), cudaMemcpyHostToDevice);
-    cudaMemset(w->tile_part, 0, 8 * (size_t)R_KINDS * T);
-    cudaMemset(w->mctl, 0, 4 * (6 * (size_t)nmem + 2));
+    // uploads on the caller's stream, never the legacy default stream (pageable sources are
+    // staged before each call returns)
+    cudaMemcpyAsync(w->tile_r0, tr0.data(), 4 * T, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(w->tile_r1, tr1.data(), 4 * T, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(w->tile_mem, tm.data(), 4 * T, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(w->mem_t0, mt0.data(), 4 * nmem, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(w->mem_t1, mt1.data(), 4 * nmem, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(w->blk64, b64.data(), 4 * b64.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(w->blkir, bir.data(), 4 * bir.size(), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(w->tile_part, 0, 8 * (size_t)R_KINDS * T, st);
+    cudaMemsetAsync(w->mctl, 0, 4 * (6 * (size_t)nmem + 2), st);
+    cudaStreamSynchronize(st);
     return cudaGetLastError();
 }
 

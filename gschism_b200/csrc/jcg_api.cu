@@ -80,7 +80,7 @@ template <typename T>
 static cudaError_t jalloc(gs_jcg* s, T*& p, size_t n) {
     void* q = nullptr;
     cudaError_t e = cudaMalloc(&q, (n ? n : 1) * sizeof(T));
-    if (e == cudaSuccess) { cudaMemset(q, 0, (n ? n : 1) * sizeof(T)); s->allocs.push_back(q); p = (T*)q; }
+    if (e == cudaSuccess) { cudaMemsetAsync(q, 0, (n ? n : 1) * sizeof(T), s->st); s->allocs.push_back(q); p = (T*)q; }
     return e;
 }
 
@@ -99,7 +99,8 @@ gs_status gs_jcg_create(int n, int nnz, int precision, int device, gs_jcg** out)
     J(scratch, 2); J(ir32, (size_t)kIrVectors * n); J(diag32, n);
     J(bar, 2); J(err, 1);
 #undef J
-    if (e == cudaSuccess) e = jcg_work_alloc(s->w, std::vector<int>{0}, std::vector<int>{n}, false);
+    if (e == cudaSuccess) e = jcg_work_alloc(s->w, std::vector<int>{0}, std::vector<int>{n}, false, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
     if (e != cudaSuccess) {
         gs_status st = (e == cudaErrorMemoryAllocation) ? GS_ERR_OOM : GS_ERR_CUDA;
         gs_jcg_destroy(s);
@@ -144,10 +145,12 @@ gs_status gs_jcg_solve_csr(gs_jcg* s, double rtol, int maxiter, int check_every,
     e = jcg_read_iters(s->w, it, outer, s->st);
     if (e != cudaSuccess) { s->msg = cudaGetErrorString(e); return GS_ERR_CUDA; }
     int32_t flags = 0;
-    cudaMemcpy(&flags, s->err, 4, cudaMemcpyDeviceToHost);
+    cudaMemcpyAsync(&flags, s->err, 4, cudaMemcpyDeviceToHost, s->st);
+    cudaStreamSynchronize(s->st);
     if (iters) *iters = it[0];
     if (flags & ERR_BARRIER_TIMEOUT) {
-        cudaMemset(s->bar, 0, sizeof(unsigned));     // the barrier word is left mid-round
+        cudaMemsetAsync(s->bar, 0, sizeof(unsigned), s->st);     // the barrier word is left mid-round
+        cudaStreamSynchronize(s->st);
         s->msg = "device barrier timed out";
         return GS_ERR_TIMEOUT;
     }

@@ -166,7 +166,13 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
         for (int e = gid; e < NE; e += G) {
             const int m = d.elem_member[e];
             const double rem = ((volatile double*)T.rem)[par * nmem + m];
-            if (!(rem > 0.0)) continue;
+            if (!(rem > 0.0)) {
+                // a finished member stays finished: carry its remaining time into the next
+                // parity slot, which otherwise still holds its value from before its last
+                // sub-step and would make it run (and leave the count of active members) again
+                if (e == d.mem_ne0[m]) T.rem[nxt * nmem + m] = rem;
+                continue;
+            }
             const double mdt = __longlong_as_double((long long)((volatile unsigned long long*)T.mindt)[par * nmem + m]);
             const double dtb = fmin(rem, mdt);
             const bool last = !((rem - dtb) > 0.0);

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -48,6 +49,17 @@ struct HostBatch {
     std::vector<double> tr, etr;         // [ntr][nvrt][NP], [ntr][nvrt][NE]
 };
 
+// Host-side result of gs_ctx_prepare, consumed (and released) by gs_ctx_finalize.
+struct Prepared {
+    HostBatch B;
+    int NP = 0, NE = 0, NS = 0;
+    std::vector<int32_t> en, es;          // [3][NE]
+    std::vector<double> gphi;             // [3][NE][2]
+    std::vector<int8_t> ssg;              // [3][NE]
+    std::vector<int2> sell;               // SELL-32 slices
+    std::vector<int32_t> sidx;            // SELL entries' columns
+};
+
 }  // namespace
 
 struct gs_ctx {
@@ -75,6 +87,7 @@ struct gs_ctx {
     // storm parameters per member ([nmem][kVortexParams]) and how many members have one
     std::vector<double> h_vort;
     int nvortex = 0;
+    Prepared* prep = nullptr;        // host preparation awaiting gs_ctx_finalize
     gs_status fail(gs_status s, const std::string& m) { err = m; return s; }
 };
 
@@ -84,14 +97,14 @@ template <typename T>
 cudaError_t dalloc(gs_ctx* c, T*& p, size_t n) {
     void* q = nullptr;
     cudaError_t e = cudaMalloc(&q, (n ? n : 1) * sizeof(T));
-    if (e == cudaSuccess) { cudaMemset(q, 0, (n ? n : 1) * sizeof(T)); c->allocs.push_back(q); p = (T*)q; }
+    if (e == cudaSuccess) { cudaMemsetAsync(q, 0, (n ? n : 1) * sizeof(T), c->own_st); c->allocs.push_back(q); p = (T*)q; }
     return e;
 }
 
 template <typename T>
 cudaError_t dup(gs_ctx* c, T*& p, const std::vector<T>& h) {
     cudaError_t e = dalloc(c, p, h.size());
-    if (e == cudaSuccess && !h.empty()) e = cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !h.empty()) e = cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->own_st);
     return e;
 }
 
@@ -322,18 +335,13 @@ static gs_status build_member(gs_ctx* c, MemberHost& m, HostBatch& B, int mid) {
     return GS_OK;
 }
 
-extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
-    if (!c || c->finalized) return GS_ERR_ARG;
-    if (c->mem.empty()) return c->fail(GS_ERR_ARG, "no members");
-    cudaError_t ce = cudaSetDevice(c->cfg.device);
-    if (ce != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(ce));
-    c->dev = c->cfg.device;
-    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
-    int coop = 0;
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->dev);
-    if (!coop) return c->fail(GS_ERR_CUDA, "device lacks cooperative launch");
+// Host half of finalize: connectivity, space-filling-curve order, batch arrays, matrix layout and
+// element geometry, with no CUDA call, so it can run on any thread while the GPU is busy.
+static gs_status prepare_host(gs_ctx* c) {
     const int nvrt = c->cfg.nvrt, ntr = c->cfg.ntr;
-    HostBatch B;
+    Prepared* pr = new Prepared();
+    std::unique_ptr<Prepared> guard(pr);
+    HostBatch& B = pr->B;
     B.nne_s.push_back(0); B.nnp_s.push_back(0); B.indptr.push_back(0);
     for (size_t k = 0; k < c->mem.size(); k++) {
         B.mem_np0.push_back((int)B.x.size());
@@ -342,12 +350,17 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
         if (s != GS_OK) return s;
     }
     const int NP = (int)B.x.size(), NE = (int)B.area.size(), NS = (int)B.len.size();
+    pr->NP = NP; pr->NE = NE; pr->NS = NS;
     B.mem_np0.push_back(NP); B.mem_ne0.push_back(NE);
     // second halves of [2][NS] and the [3][NE] arrays, geometry of elements, initial tracers
     std::vector<int32_t> sn2(NS), se2(NS);
-    std::vector<int32_t> en(3 * (size_t)NE), es(3 * (size_t)NE);
-    std::vector<double> gphi(6 * (size_t)NE);
-    std::vector<int8_t> ssg(3 * (size_t)NE);
+    std::vector<int32_t>& en = pr->en;
+    std::vector<int32_t>& es = pr->es;
+    std::vector<double>& gphi = pr->gphi;
+    std::vector<int8_t>& ssg = pr->ssg;
+    en.assign(3 * (size_t)NE, 0); es.assign(3 * (size_t)NE, 0);
+    gphi.assign(6 * (size_t)NE, 0.0);
+    ssg.assign(3 * (size_t)NE, 0);
     B.tr.assign((size_t)ntr * nvrt * NP, 0.0);
     B.etr.assign((size_t)ntr * nvrt * NE, 0.0);
     for (auto& m : c->mem) {
@@ -392,11 +405,9 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     B.sn.insert(B.sn.end(), sn2.begin(), sn2.end());
     B.se.insert(B.se.end(), se2.begin(), se2.end());
 
-    // ------------------------------------------------------------------ device state
-    Dev& d = c->d;
     // SELL-32 layout of the batch matrix; assembly slots move to their SELL positions
-    std::vector<int2> sell;
-    std::vector<int32_t> sidx;
+    std::vector<int2>& sell = pr->sell;
+    std::vector<int32_t>& sidx = pr->sidx;
     {
         const int nsl = (NP + 31) / 32;
         sell.resize(nsl);
@@ -428,6 +439,46 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
         c->h_indptr = B.indptr;
         c->h_indices = B.indices;
     }
+    c->prep = guard.release();
+    return GS_OK;
+}
+
+extern "C" gs_status gs_ctx_prepare(gs_ctx* c) {
+    if (!c || c->finalized) return GS_ERR_ARG;
+    if (c->prep) return GS_OK;
+    if (c->mem.empty()) return c->fail(GS_ERR_ARG, "no members");
+    return prepare_host(c);
+}
+
+extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
+    if (!c || c->finalized) return GS_ERR_ARG;
+    if (c->mem.empty()) return c->fail(GS_ERR_ARG, "no members");
+    if (!c->prep) {
+        const gs_status ps = prepare_host(c);
+        if (ps != GS_OK) return ps;
+    }
+    std::unique_ptr<Prepared> pr(c->prep);     // released when finalize returns
+    c->prep = nullptr;
+    cudaError_t ce = cudaSetDevice(c->cfg.device);
+    if (ce != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(ce));
+    c->dev = c->cfg.device;
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->dev);
+    if (!coop) return c->fail(GS_ERR_CUDA, "device lacks cooperative launch");
+    // uploads, clears and set-up kernels go to the context's own non-blocking stream
+    if (cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking) != cudaSuccess) return c->fail(GS_ERR_CUDA, "stream");
+    c->st = c->own_st;
+    const int nvrt = c->cfg.nvrt, ntr = c->cfg.ntr;
+    HostBatch& B = pr->B;
+    const int NP = pr->NP, NE = pr->NE, NS = pr->NS;
+    const std::vector<int32_t>& en = pr->en;
+    const std::vector<int32_t>& es = pr->es;
+    const std::vector<double>& gphi = pr->gphi;
+    const std::vector<int8_t>& ssg = pr->ssg;
+    const std::vector<int2>& sell = pr->sell;
+    const std::vector<int32_t>& sidx = pr->sidx;
+    Dev& d = c->d;
     d.NP = NP; d.NE = NE; d.NS = NS; d.NNZ = (int)sidx.size(); d.NB = (int)B.bn_node.size();
     d.nmem = (int)c->mem.size();
     cudaError_t e = cudaSuccess;
@@ -451,7 +502,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     AL(zc, (size_t)nvrt * NS); AL(Qh, (size_t)nvrt * NS); AL(su2, (size_t)nvrt * NS); AL(btu, (size_t)nvrt * NS);
     AL(btel, (size_t)nvrt * NS); AL(U, NS); AL(gE1, NS); AL(gE2, NS); AL(hhat, NS); AL(chi, NS); AL(chi2, NS);
     UP(en, en); UP(es, es); UP(area, B.area);
-    if (e == cudaSuccess) { e = dalloc(c, d.gphi, 3 * (size_t)NE); if (e == cudaSuccess) e = cudaMemcpy(d.gphi, gphi.data(), gphi.size() * 8, cudaMemcpyHostToDevice); }
+    if (e == cudaSuccess) { e = dalloc(c, d.gphi, 3 * (size_t)NE); if (e == cudaSuccess) e = cudaMemcpyAsync(d.gphi, gphi.data(), gphi.size() * 8, cudaMemcpyHostToDevice, c->own_st); }
     UP(ssgn, ssg); AL(kbe, NE); AL(edry, NE);
     AL(ez, (size_t)nvrt * NE); AL(ew, (size_t)nvrt * NE); AL(Qv, (size_t)nvrt * NE);
     UP(etr, B.etr); AL(prev, (size_t)ntr * nvrt * NE); AL(maxDt, NE); AL(ghat, NE);
@@ -466,7 +517,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     {
         std::vector<int> row0, rows;
         for (auto& m : c->mem) { row0.push_back(m.np0); rows.push_back(m.np); }
-        e = jcg_work_alloc(c->jw, row0, rows, true);
+        e = jcg_work_alloc(c->jw, row0, rows, true, c->own_st);
         if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
     }
     // constants
@@ -486,8 +537,6 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
         vg.cs[k] = (1.0 - tb) * std::sinh(tf * s) / std::sinh(tf) +
                    tb * (std::tanh(tf * (s + 0.5)) - std::tanh(tf * 0.5)) / 2.0 / std::tanh(tf * 0.5);
     }
-    if (cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking) != cudaSuccess) return c->fail(GS_ERR_CUDA, "stream");
-    c->st = c->own_st;
     // cold start levels (schism_init.py:81-91)
     launch_levels(c->d, c->P, c->vg, 0, c->st, c->nsm);
     e = cudaStreamSynchronize(c->st);
@@ -644,9 +693,10 @@ gs_status gs_get_stats(gs_ctx* c, int member, gs_stats* out) {
     if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
     unsigned long long cnt[4] = {0, 0, 0, 0};
     int32_t nsub = 0, flags = 0;
-    cudaMemcpy(cnt, c->d.counters, sizeof(cnt), cudaMemcpyDeviceToHost);
-    cudaMemcpy(&nsub, c->d.mem_nsub + member, 4, cudaMemcpyDeviceToHost);
-    cudaMemcpy(&flags, c->d.err, 4, cudaMemcpyDeviceToHost);
+    cudaMemcpyAsync(cnt, c->d.counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->st);
+    cudaMemcpyAsync(&nsub, c->d.mem_nsub + member, 4, cudaMemcpyDeviceToHost, c->st);
+    cudaMemcpyAsync(&flags, c->d.err, 4, cudaMemcpyDeviceToHost, c->st);
+    cudaStreamSynchronize(c->st);
     std::memset(out, 0, sizeof(*out));
     out->jcg_iters = iters[member];
     out->jcg_outer = outer[member];
@@ -659,6 +709,7 @@ gs_status gs_get_stats(gs_ctx* c, int member, gs_stats* out) {
 
 gs_status gs_ctx_destroy(gs_ctx* c) {
     if (!c) return GS_ERR_ARG;
+    delete c->prep;
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->own_st) cudaStreamDestroy(c->own_st);
@@ -767,7 +818,8 @@ extern "C" gs_status gs_state_get(gs_ctx* c, int member, int field, void* host, 
         } else {
             if (bytes != 8 * src.size()) return c->fail(GS_ERR_STATE, "size");
             std::vector<double> all(c->d.NNZ);
-            cudaMemcpy(all.data(), c->d.A, 8 * (size_t)c->d.NNZ, cudaMemcpyDeviceToHost);
+            cudaMemcpyAsync(all.data(), c->d.A, 8 * (size_t)c->d.NNZ, cudaMemcpyDeviceToHost, c->st);
+            cudaStreamSynchronize(c->st);
             double* out = (double*)host;
             for (size_t a = 0; a < src.size(); a++) out[a] = all[src[a]];
         }
@@ -788,7 +840,8 @@ extern "C" gs_status gs_state_get(gs_ctx* c, int member, int field, void* host, 
     for (int t = 0; t < nt; t++)
         for (int k = 0; k < nl; k++) {
             const size_t dev_off = (((size_t)t * nl + k) * N + off) * nc * dsz;
-            cudaMemcpy(buf.data(), (char*)fi.ptr + dev_off, buf.size(), cudaMemcpyDeviceToHost);
+            cudaMemcpyAsync(buf.data(), (char*)fi.ptr + dev_off, buf.size(), cudaMemcpyDeviceToHost, c->st);
+            cudaStreamSynchronize(c->st);
             for (int i = 0; i < n; i++) {
                 const int o = perm[i];
                 const size_t dst = ((((size_t)t * nl + k) * n + o) * nc) * esz;
@@ -831,7 +884,8 @@ extern "C" gs_status gs_state_put(gs_ctx* c, int member, int field, const void* 
                 else std::memcpy(buf.data() + (size_t)i * nc * dsz, (const char*)host + src, nc * dsz);
             }
             const size_t dev_off = (((size_t)t * nl + k) * N + off) * nc * dsz;
-            cudaMemcpy((char*)fi.ptr + dev_off, buf.data(), buf.size(), cudaMemcpyHostToDevice);
+            cudaMemcpyAsync((char*)fi.ptr + dev_off, buf.data(), buf.size(), cudaMemcpyHostToDevice, c->st);
+            cudaStreamSynchronize(c->st);
         }
     return GS_OK;
 }

@@ -59,7 +59,10 @@ def _flat(segs):
 class Model:
     def __init__(self, cases: Sequence[Case], precision: str = "fp64", device: int = 0,
                  rtol: float | None = None, maxiter: int | None = None, check_every: int | None = None,
-                 ir_inner_rtol: float = 0.1, ir_inner_maxiter: int = 400):
+                 ir_inner_rtol: float = 0.1, ir_inner_maxiter: int = 400, defer_device: bool = False):
+        """A batch context of `cases`.  With defer_device the constructor only does the host
+        preparation (gs_ctx_prepare, no CUDA call: fit for a worker thread) and finalize() later
+        allocates and uploads the device state."""
         self.lib = L.load()
         self.cases: List[Case] = list(cases)
         c0 = self.cases[0]
@@ -89,14 +92,25 @@ class Model:
         self.h = h
         for c in self.cases:
             self._add(c)
+        self.nvrt, self.ntr = vg.nvrt, c0.ntracers
+        self.sizes = None
+        if defer_device:
+            L.check(self.lib.gs_ctx_prepare(self.h), self.h, "gs_ctx_prepare")
+        else:
+            self.finalize()
+
+    def finalize(self) -> None:
+        """Device half of the set-up (gs_ctx_finalize); a no-op once done."""
+        if self.sizes is not None:
+            return
         L.check(self.lib.gs_ctx_finalize(self.h), self.h, "gs_ctx_finalize")
-        self.sizes = []
+        sizes = []
         for m in range(len(self.cases)):
             a, b, cc, d = (ctypes.c_int() for _ in range(4))
             L.check(self.lib.gs_member_sizes(self.h, m, ctypes.byref(a), ctypes.byref(b), ctypes.byref(cc),
                                              ctypes.byref(d)), self.h)
-            self.sizes.append(dict(np=a.value, ne=b.value, ns=cc.value, nnz=d.value))
-        self.nvrt, self.ntr = vg.nvrt, c0.ntracers
+            sizes.append(dict(np=a.value, ne=b.value, ns=cc.value, nnz=d.value))
+        self.sizes = sizes
 
     def _k(self, a, dt):
         a = np.ascontiguousarray(a, dtype=dt)

@@ -6,17 +6,20 @@ Requests (a mesh with its forcing and a horizon in steps) arrive over time.  The
 FIFO queue and, at every scheduling turn, admits the longest prefix of the queue whose device
 memory (`footprint_bytes`, an upper bound of what the context allocates) fits in the memory left
 by the running work: the admitted requests become one cohort, a batch context holding them all
-as members.  New cohorts are built on a worker thread (host preprocessing and upload) while the
-running cohorts keep stepping, and join the stepping as soon as they are built.  Every turn
+as members.  A new cohort's host preparation (connectivity, ordering, matrix layout: the bulk of
+the set-up, no CUDA call) runs on worker threads while the running cohorts keep stepping; its
+device half (allocation, upload, cold start: well under a second) runs on the stepping thread
+between two turns, so building never competes with stepping on the device.  Every turn
 advances each running cohort by a few steps; a cohort whose requests reach their horizon hands
 back its results, releases its memory and leaves.  So requests that arrive while others run are
 admitted as memory frees up and their steps interleave with the running ones, turn by turn.
 
-All cohorts step on one CUDA stream: the step's persistent kernels (elevation solve, transport)
-wait on each other's blocks and are never run concurrently with another such kernel.  Only the
-regular kernels of a cohort being built overlap them.  A member's results do not depend on the
-batch it runs in (per-member reductions in a fixed order), so each forecast is the same alone
-and in the mix.
+Every turn a cohort advances about the same number of node-steps (a 2M-node forecast one step,
+a 30k-node one dozens), so the GPU is shared among the running forecasts and short ones finish
+early.  All cohorts step on one CUDA stream: the step's persistent kernels (elevation solve,
+transport) wait on each other's blocks and are never run concurrently with another such kernel.
+A member's results do not depend on the batch it runs in (per-member reductions in a fixed
+order), so each forecast is the same alone and in the mix.
 
 Reported: time-to-forecast per request (arrival to results on the host), its p50/p99, and the
 node-level-steps/s of the whole run.
@@ -76,15 +79,21 @@ class ModelEngine:
         return int(self.torch.cuda.mem_get_info(self.device)[0])
 
     def build(self, reqs: Sequence[Request]):
+        """Host preparation only (worker thread): no CUDA call, so it never competes with the
+        running steps for the device."""
         from .model import Model
+        return Model([r.case for r in reqs], precision=self.precision, device=self.device, defer_device=True)
+
+    def activate(self, h, reqs: Sequence[Request]) -> None:
+        """Device half on the stepping thread, between turns: allocation, upload, cold start,
+        storm forcing, and the shared stream."""
         self.torch.cuda.set_device(self.device)
-        m = Model([r.case for r in reqs], precision=self.precision, device=self.device)
+        h.finalize()
         for i, r in enumerate(reqs):
             if r.vortex is not None:
-                m.set_vortex(i, r.vortex)
-        m.sync()
-        m.set_stream(self.stream.cuda_stream)
-        return m
+                h.set_vortex(i, r.vortex)
+        h.sync()
+        h.set_stream(self.stream.cuda_stream)
 
     def advance(self, h, k: int) -> None:
         h.step(k)
@@ -115,15 +124,18 @@ class Server:
     """Continuous-batching scheduler over an engine (see the module docstring)."""
 
     def __init__(self, engine, budget_bytes: Optional[int] = None, max_members: int = 64,
-                 steps_per_turn: int = 8, background_build: bool = True,
+                 steps_per_turn: int = 8, turn_node_steps: Optional[int] = 2_000_000, build_workers: int = 2,
+                 background_build: bool = True,
                  clock: Callable[[], float] = time.perf_counter, sleep: Callable[[float], None] = time.sleep,
                  on_finish: Optional[Callable[[Request], None]] = None):
         self.engine = engine
         self.budget = int(budget_bytes if budget_bytes is not None else 0.9 * engine.free_bytes())
         self.max_members = max_members
         self.steps_per_turn = max(1, steps_per_turn)
+        self.turn_node_steps = turn_node_steps
         self.clock, self.sleep = clock, sleep
-        self.pool = cf.ThreadPoolExecutor(max_workers=1) if background_build else None
+        self.pool = cf.ThreadPoolExecutor(max_workers=max(1, build_workers)) if background_build else None
+        self._t0 = 0.0
         self.used = 0
         self.peak_used = 0
         self.log: List[tuple] = []
@@ -158,18 +170,33 @@ class Server:
         self.peak_used = max(self.peak_used, self.used)
         c = _Cohort(cid=cid, reqs=group, nbytes=nbytes, target=group[0].nsteps)
         if self.pool is not None:
-            c.future = self.pool.submit(self.engine.build, group)
+            c.future = self.pool.submit(self._build, cid, group)
         else:
-            c.handle = self.engine.build(group)
+            c.handle = self._build(cid, group)
         self.log.append(("admit", now, cid, [r.rid for r in group], nbytes))
         return c
+
+    def _turn_steps(self, c: _Cohort) -> int:
+        """Steps a cohort advances in one turn: about turn_node_steps node-steps (a large cohort
+        one step, a small one many), so every running forecast gets a similar share of the GPU per
+        turn and short ones finish early; steps_per_turn when no share is set."""
+        if not self.turn_node_steps:
+            return self.steps_per_turn
+        nodes = sum(int(r.case.n_nodes) for r in c.reqs)
+        return max(1, int(self.turn_node_steps // max(1, nodes)))
+
+    def _build(self, cid: int, group: Sequence[Request]):
+        t = self.clock()
+        h = self.engine.build(group)
+        self.log.append(("build", cid, t - self._t0, self.clock() - t))
+        return h
 
     def run(self, requests: Sequence[Request]) -> List[Request]:
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
         queue: List[Request] = []
         building: List[_Cohort] = []
         active: List[_Cohort] = []
-        t0 = self.clock()
+        t0 = self._t0 = self.clock()
         cid = 0
         try:
             while pending or queue or building or active:
@@ -188,6 +215,10 @@ class Server:
                         if not c.future.done():
                             continue
                         c.handle = c.future.result()
+                    ta = self.clock()
+                    if hasattr(self.engine, "activate"):
+                        self.engine.activate(c.handle, c.reqs)
+                    self.log.append(("activate", c.cid, ta - t0, self.clock() - ta))
                     building.remove(c)
                     active.append(c)
                     t = self.clock() - t0
@@ -200,11 +231,13 @@ class Server:
                         waits.append(pending[0].arrival - now)
                     self.sleep(max(0.0, min(waits)) if waits else 0.002)
                     continue
+                tt = self.clock()
                 for c in active:
-                    k = min(self.steps_per_turn, c.target - c.done)
+                    k = min(self._turn_steps(c), c.target - c.done)
                     self.engine.advance(c.handle, k)
                     c.done += k
                 self.engine.wait()
+                self.log.append(("turn", tt - t0, self.clock() - tt, len(active)))
                 for c in list(active):
                     if c.done < c.target:
                         continue

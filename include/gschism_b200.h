@@ -94,6 +94,10 @@ typedef struct gs_ctx gs_ctx;
 
 gs_status gs_ctx_create(const gs_config* cfg, gs_ctx** out);
 gs_status gs_member_add(gs_ctx* ctx, const gs_member_desc* desc, int* member_id);
+/* Host half of gs_ctx_finalize: connectivity, space-filling-curve order, matrix layout and
+ * geometry of every added member, with no CUDA call (so it can run on a worker thread while the
+ * GPU steps other contexts).  Optional: gs_ctx_finalize runs it when it has not been run. */
+gs_status gs_ctx_prepare(gs_ctx* ctx);
 /* Allocate device state for every added member, upload, build geometry and cold-start levels. */
 gs_status gs_ctx_finalize(gs_ctx* ctx);
 gs_status gs_ctx_destroy(gs_ctx* ctx);

@@ -199,3 +199,36 @@ def test_member_at_rest_beside_a_forced_one(native, precision):
     alone.step(3)
     assert np.array_equal(mix.get(1, "ETA2"), alone.get(0, "ETA2"))
     assert mix.stats(1)["jcg_iters"] == alone.stats(0)["jcg_iters"]
+
+
+def test_transport_members_with_different_substep_counts(native):
+    """Members of one batch that need different numbers of transport sub-steps (one many, one a
+    single sub-step): the sub-cycling ends, and each member's tracers equal those of the same
+    member alone (a member that finished early must stay finished)."""
+    from gschism_b200.model import Model
+    a = cases.channel(seed=61, nx=30, ny=16)
+    b = cases.channel(seed=62, nx=40, ny=21)
+    for c in (a, b):
+        c.params.dramp = 0.0              # full tide from the first step: real flow by step 3
+    before = ["BTRACK", "PREPARE", "ASSEMBLE", "SOLVE", "UPDATE_ELEV", "MOMENTUM", "VVEL"]
+
+    def third_step(m, scaled):
+        m.step(2)
+        m.phase("BEGIN", 3)
+        for ph in before:
+            m.phase(ph, 3)
+        for k in scaled:                      # 50x the fluxes: many more transport sub-steps
+            qh = m.get(k, "SIDE_QH")
+            m.put(k, "SIDE_QH", np.where(qh > -1e30, 50.0 * qh, qh))
+        m.phase("TRANSPORT", 3)
+        m.sync()
+
+    mix = Model([a, b])
+    third_step(mix, [0])
+    alone_a, alone_b = Model([a]), Model([b])
+    third_step(alone_a, [0])
+    third_step(alone_b, [])
+    assert mix.stats(0)["transport_substeps"] >= 3
+    assert mix.stats(1)["transport_substeps"] == 1
+    assert np.array_equal(mix.get(0, "ELEM_TR"), alone_a.get(0, "ELEM_TR"))
+    assert np.array_equal(mix.get(1, "ELEM_TR"), alone_b.get(0, "ELEM_TR"))

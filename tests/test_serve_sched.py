@@ -115,3 +115,14 @@ def test_request_larger_than_budget_is_an_error():
     reqs = [Request(rid=0, case=_case(1_000_000), nsteps=4, arrival=0.0)]
     with pytest.raises(RuntimeError):
         _run(reqs, budget=1000)
+
+
+def test_turn_share_by_node_steps():
+    clk = Clock()
+    srv = Server(FakeEngine(clk), budget_bytes=10**9, turn_node_steps=2_000_000, background_build=False,
+                 clock=clk, sleep=clk.sleep)
+    from gschism_b200.serve import _Cohort
+    big = _Cohort(cid=0, reqs=[Request(rid=0, case=_case(2_000_000), nsteps=10)], nbytes=0, target=10)
+    small = _Cohort(cid=1, reqs=[Request(rid=1, case=_case(25_000), nsteps=10)], nbytes=0, target=10)
+    assert srv._turn_steps(big) == 1
+    assert srv._turn_steps(small) == 80
