@@ -125,6 +125,7 @@ class Server:
 
     def __init__(self, engine, budget_bytes: Optional[int] = None, max_members: int = 64,
                  steps_per_turn: int = 8, turn_node_steps: Optional[int] = 2_000_000, build_workers: int = 2,
+                 max_cohort_nodes: int = 1_000_000,
                  background_build: bool = True,
                  clock: Callable[[], float] = time.perf_counter, sleep: Callable[[float], None] = time.sleep,
                  on_finish: Optional[Callable[[Request], None]] = None):
@@ -133,6 +134,7 @@ class Server:
         self.max_members = max_members
         self.steps_per_turn = max(1, steps_per_turn)
         self.turn_node_steps = turn_node_steps
+        self.max_cohort_nodes = max_cohort_nodes
         self.clock, self.sleep = clock, sleep
         self.pool = cf.ThreadPoolExecutor(max_workers=max(1, build_workers)) if background_build else None
         self._t0 = 0.0
@@ -142,12 +144,17 @@ class Server:
         self.on_finish = on_finish
 
     def _admit(self, queue: List[Request], now: float, cid: int) -> Optional[_Cohort]:
-        """Longest FIFO prefix of same-horizon requests that fits in the free budget."""
+        """Longest FIFO prefix of same-horizon requests that fits in the free budget and in
+        max_cohort_nodes (a request above it gets a cohort of its own, so small forecasts neither
+        wait for its set-up nor step at its pace)."""
         if not queue:
             return None
         group: List[Request] = []
         nbytes = 0
+        nodes = 0
         for r in queue:
+            if group and nodes + int(r.case.n_nodes) > self.max_cohort_nodes:
+                break
             if group and (r.nsteps != group[0].nsteps or r.case.vgrid.nvrt != group[0].case.vgrid.nvrt
                           or r.case.ntracers != group[0].case.ntracers or r.case.params.dt != group[0].case.params.dt):
                 break
@@ -158,6 +165,7 @@ class Server:
                 break
             group.append(r)
             nbytes = nb
+            nodes += int(r.case.n_nodes)
         if not group:
             if self.used == 0:
                 raise RuntimeError(f"request {queue[0].rid} needs more device memory than the budget")

@@ -126,3 +126,12 @@ def test_turn_share_by_node_steps():
     small = _Cohort(cid=1, reqs=[Request(rid=1, case=_case(25_000), nsteps=10)], nbytes=0, target=10)
     assert srv._turn_steps(big) == 1
     assert srv._turn_steps(small) == 80
+
+
+def test_large_request_gets_its_own_cohort():
+    reqs = [Request(rid=0, case=_case(2_000_000), nsteps=8, arrival=0.0)]
+    reqs += [Request(rid=i, case=_case(20_000), nsteps=8, arrival=0.0) for i in range(1, 4)]
+    srv, eng, clk = _run(reqs, budget=10**12)
+    assert reqs[0].cohort != reqs[1].cohort
+    assert reqs[1].cohort == reqs[2].cohort == reqs[3].cohort
+    assert all(r.finished < reqs[0].finished for r in reqs[1:])
