@@ -32,6 +32,19 @@ enum : int {
     ERR_DEGREE = 4,
 };
 
+// Static geometry of one element for the backtracking gathers: the corner positions and node ids
+// in element node order, the area, and in perm which node starts each of the element's sides in
+// the element's orientation (bits 2j..2j+1 for side j) and whether sides j and j+1 meet at an
+// obtuse corner (bit 8+j).  One 80-byte record replaces the side -> node -> x/y chains of
+// dependent loads of the walk and the interpolation.
+struct alignas(16) ElemGeo {
+    double2 p[3];
+    double area;
+    int32_t n[3];
+    int32_t perm;
+};
+static_assert(sizeof(ElemGeo) == 80, "ElemGeo layout");
+
 // Batch-wide constants shared by all members (copied into kernel arguments).
 struct Phys {
     int nvrt, ntr, nz;
@@ -82,6 +95,7 @@ struct Dev {
     double *hhat, *chi, *chi2;
     // elements
     int32_t *en, *es;              // [3][NE]
+    ElemGeo* egeo;                 // [NE]
     double *area;
     double2 *gphi;                 // [3][NE]
     int8_t *ssgn;                  // [3][NE]

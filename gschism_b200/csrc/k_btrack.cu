@@ -15,54 +15,51 @@ namespace {
 constexpr double kSmall = 1.0e-7;
 constexpr int kWalkMax = 40;
 
-struct BtCtx {
-    const Dev& d;
-    const VG& vg;
-};
-
 __device__ __forceinline__ double2 npos(const Dev& d, int i) { return v2(d.x[i], d.y[i]); }
 
 __device__ __forceinline__ double signed_area(double2 p1, double2 p2, double2 p3) {
     return 0.5 * ((p1.x - p3.x) * (p2.y - p3.y) - (p2.x - p3.x) * (p1.y - p3.y));
 }
 
-__device__ __forceinline__ int node_in_order(const Dev& d, int e, int idx) {
-    const int s = d.es[idx * d.NE + e];
-    return (d.ssgn[idx * d.NE + e] > 0) ? d.sn[s] : d.sn[d.NS + s];
+__device__ __forceinline__ double2 corner(const double2 (&p)[3], int j) {
+    return j == 0 ? p[0] : (j == 1 ? p[1] : p[2]);
 }
 
-__device__ unsigned valid_exits(const Dev& d, int e, double2 x0, double2 xt, double& fac) {
-    double2 C[4];
-    C[0] = npos(d, node_in_order(d, e, 0));
-    C[1] = npos(d, node_in_order(d, e, 1));
-    C[2] = npos(d, node_in_order(d, e, 2));
-    C[3] = C[2];
+// Exits of element e through which the walk from x0 towards xt may leave (one bit per side, in
+// the element's side order); 0 when xt is inside.  The corners are taken in the element's
+// orientation: corner j starts side j.  Of the reference's four-corner predicate masks only the
+// three triangle bits can be set (its fourth "left" bit is always set, which masks the rest), and
+// the obtuse-corner bits depend on the element alone, so they come with the element record.
+__device__ unsigned valid_exits(const ElemGeo* geo, int e, double2 x0, double2 xt, double& fac) {
+    double2 p[3];
+    p[0] = geo[e].p[0]; p[1] = geo[e].p[1]; p[2] = geo[e].p[2];
+    const int pm = geo[e].perm;
+    double2 C[3];
+    C[0] = corner(p, pm & 3);
+    C[1] = corner(p, (pm >> 2) & 3);
+    C[2] = corner(p, (pm >> 4) & 3);
     const double2 vt0 = xt - x0;
     double mp = fmax(dot2(vt0, C[0] - x0), dot2(vt0, C[1] - x0));
     mp = fmax(mp, dot2(vt0, C[2] - x0));
     fac = fmax(1.00001 * fac, fmin(1.0, (mp / dot2(vt0, vt0)) * 1.00001));
     const double2 ixt = x0 + (xt - x0) * fac;
-    const double2 s0 = C[1] - C[0], s1 = C[2] - C[1], s2 = C[0] - C[2], s3 = C[0] - C[0];
-    unsigned left = 8u, obt = 0u, bis = 0u;
+    const double2 s0 = C[1] - C[0], s1 = C[2] - C[1], s2 = C[0] - C[2];
+    unsigned left = 0u, bis = 0u;
     left |= (unsigned)(cross2(s0, ixt - C[0]) > -kSmall);
     left |= (unsigned)(cross2(s1, ixt - C[1]) > -kSmall) << 1;
     left |= (unsigned)(cross2(s2, ixt - C[2]) > -kSmall) << 2;
-    obt |= (unsigned)(dot2(s0, s1) > 0.0);
-    obt |= (unsigned)(dot2(s1, s2) > 0.0) << 1;
-    obt |= (unsigned)(dot2(s2, s0) > 0.0) << 2;
-    obt |= (unsigned)(dot2(s3, s0) > 0.0) << 3;
+    const unsigned obt = (unsigned)(pm >> 8) & 7u;
     bis |= (unsigned)(dot2(ixt - C[1], s0 + s1) < 0.0);
     bis |= (unsigned)(dot2(ixt - C[2], s1 + s2) < 0.0) << 1;
     bis |= (unsigned)(dot2(ixt - C[0], s2 + s0) < 0.0) << 2;
-    bis |= (unsigned)(dot2(ixt - C[0], s3 + s0) < 0.0) << 3;
-    return (~left & 0xFu) & ((~obt & 0xFu) | bis);
+    return (~left & 7u) & ((~obt & 7u) | bis);
 }
 
 // returns 1 if xt was found inside *cur, 0 if the walk stopped at a boundary or dry element
 __device__ int celestial_walk(const Dev& d, int& cur, double2 x0, double2 xt, int& lastCross) {
     double fac = 0.00001;
     for (int iter = 0; iter < kWalkMax; iter++) {
-        const unsigned valid = valid_exits(d, cur, x0, xt, fac);
+        const unsigned valid = valid_exits(d.egeo, cur, x0, xt, fac);
         if (valid == 0u) return 1;
         const int j = __ffs(valid) - 1;
         const int s = d.es[j * d.NE + cur];
@@ -76,12 +73,22 @@ __device__ int celestial_walk(const Dev& d, int& cur, double2 x0, double2 xt, in
     return 1;
 }
 
-__device__ void interp_vel(const Dev& d, const VG& vg, int e, double px, double py, double pz, double* out) {
-    const int NE = d.NE, NP = d.NP;
-    const int n0 = d.en[e], n1 = d.en[NE + e], n2 = d.en[2 * NE + e];
-    const double2 x0 = npos(d, n0), x1 = npos(d, n1), x2 = npos(d, n2);
+// Velocity at (px, py, pz) inside element e (interpolateVelocities).  The vertical bracket is
+// the pair of levels (L, L+1) with z(L) < pz <= z(L+1) of the element-interpolated level
+// heights, or the bottom (pz <= z(kbe-1)) or top (pz >= z(nvrt-1)) case.  z is non-decreasing
+// in the level (the vertical grid's levels are ordered at every wet node; a dry node's levels
+// all sit at 0 and rounding keeps a weighted sum of non-decreasing terms non-decreasing), so
+// that pair is unique and any search that keeps z(L) < pz <= z(R) ends on the same one as the
+// reference's bisection over [kbe-1, nvrt-1].  The search starts at `hint` (the previous
+// bracket of this trajectory), steps at most one level either way and bisects the rest.
+__device__ void interp_vel(const Dev& d, const VG& vg, int e, double px, double py, double pz, double* out,
+                           int& hint) {
+    const int NP = d.NP;
+    const ElemGeo& g = d.egeo[e];
+    const double2 x0 = g.p[0], x1 = g.p[1], x2 = g.p[2];
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
     const double2 xt = v2(px, py);
-    const double area = d.area[e];
+    const double area = g.area;
     double s0 = signed_area(xt, x1, x2) / area;
     double s1 = signed_area(x0, xt, x2) / area;
     double s2 = 1.0 - s0 - s1;
@@ -101,19 +108,32 @@ __device__ void interp_vel(const Dev& d, const VG& vg, int e, double px, double 
         const double z2 = compz(vg, e2, h2, kb2, k > kb2 ? k : kb2);
         return s0 * z0 + s1 * z1 + s2 * z2 + s3 * 0.0;
     };
-    int L = d.kbe[e] - 1, R = vg.nvrt - 1;
-    double zL = zat(L), zR = zat(R);
+    // L* = the highest level in [lo, hi] with z < pz (lo - 1 when there is none), searched
+    // between the sentinels lo - 1 and hi + 1: two one-level steps from the hint, then bisection
+    const int lo = d.kbe[e] - 1, hi = vg.nvrt - 1;
+    int Lk = lo - 1, Rk = hi + 1;
+    double zL = 0.0, zR = 0.0;
+    int k = min(max(hint, lo), hi);
+    for (int probe = 0; Rk - Lk > 1; probe++) {
+        const double zk = zat(k);
+        const bool below = zk < pz;
+        if (below) { Lk = k; zL = zk; } else { Rk = k; zR = zk; }
+        k = (probe < 2) ? (below ? k + 1 : k - 1) : (Lk + Rk) / 2;
+        if (k <= Lk || k >= Rk) k = (Lk + Rk) / 2;
+    }
+    hint = Lk;
+    // bottom when no level lies below pz; top when pz reaches the top height
+    int mode = (Lk < lo) ? 1 : (Lk == hi) ? 2 : 0;
+    if (mode == 0 && zR == pz && (Rk == hi || pz >= zat(hi))) mode = 2;
+    int L = Lk, R = Rk;
     double w1, w2;
-    if (pz <= zL) { w1 = 1.0; w2 = 0.0; }
-    else if (pz >= zR) { w1 = 0.0; w2 = 1.0; }
-    else {
-        while (R - L > 1) {
-            const int M = (L + R) / 2;
-            const double zM = zat(M);
-            if (zM < pz) { L = M; zL = zM; } else { R = M; zR = zM; }
-        }
+    if (mode == 0) {
         w2 = (pz - zL) / (zR - zL);
         w1 = 1.0 - w2;
+    } else {
+        L = lo; R = hi;
+        w1 = (mode == 1) ? 1.0 : 0.0;
+        w2 = 1.0 - w1;
     }
     const int kl0 = L > kb0 ? L : kb0, kl1 = L > kb1 ? L : kb1, kl2 = L > kb2 ? L : kb2;
     const int kr0 = R > kb0 ? R : kb0, kr1 = R > kb1 ? R : kb1, kr2 = R > kb2 ? R : kb2;
@@ -142,7 +162,8 @@ __device__ void side_btrack(const Dev& d, const VG& vg, const Phys& P, int s, in
     u_int[2] = 0.5 * (d.w2[(size_t)jlev * NP + a] + d.w2[(size_t)jlev * NP + b]);
     const int ea = d.se[s], eb = d.se[NS + s];
     int cur = !d.edry[ea] ? ea : eb;
-    int iter = 0;
+    int iter = 0, hint = jlev - 1;
+    bool fresh = false;   // u_int holds the interpolation at (cur, xt) of this sub-step
     double xt[3] = {-1.0e25, -1.0e25, -1.0e25};
     const double vm2 = P.velmin * P.velmin;
     for (;;) {
@@ -152,6 +173,7 @@ __device__ void side_btrack(const Dev& d, const VG& vg, const Phys& P, int s, in
         xt[2] = x0[2] - dtb * u_int[2];
         int lc = -1;
         const int found = celestial_walk(d, cur, v2(x0[0], x0[1]), v2(xt[0], xt[1]), lc);
+        fresh = false;
         if (t3 <= time_rm) { xt[0] = x0[0]; xt[1] = x0[1]; xt[2] = x0[2]; break; }
         if (!found) {
             const double2 p1 = npos(d, d.sn[lc]), p2 = npos(d, d.sn[NS + lc]);
@@ -179,12 +201,13 @@ __device__ void side_btrack(const Dev& d, const VG& vg, const Phys& P, int s, in
             const double ln = sqrt(vv.x * vv.x + vv.y * vv.y);
             const double2 tg = v2(vv.x / ln, vv.y / ln);
             double u[3];
-            interp_vel(d, vg, cur, xt[0], xt[1], xt[2], u);
+            interp_vel(d, vg, cur, xt[0], xt[1], xt[2], u, hint);
             const double dd = u[0] * tg.x + u[1] * tg.y;
             u_int[0] = tg.x * dd; u_int[1] = tg.y * dd; u_int[2] = u[2];
         } else {
             time_rm -= dtb;
-            interp_vel(d, vg, cur, xt[0], xt[1], xt[2], u_int);
+            interp_vel(d, vg, cur, xt[0], xt[1], xt[2], u_int, hint);
+            fresh = true;
         }
         if (time_rm <= 0.0) break;
         const double vmag2 = u_int[0] * u_int[0] + u_int[1] * u_int[1];
@@ -194,21 +217,28 @@ __device__ void side_btrack(const Dev& d, const VG& vg, const Phys& P, int s, in
         if (iter == 38) { atomicAdd(&d.counters[1], 1ull); elem_out = cur; return; }
         t3 = t2; t2 = t1; t1 = time_rm;
     }
-    interp_vel(d, vg, cur, xt[0], xt[1], xt[2], u_int);
+    // the final interpolation at (cur, xt); when the last sub-step ended inside an element it has
+    // just been computed with these same arguments
+    if (!fresh) interp_vel(d, vg, cur, xt[0], xt[1], xt[2], u_int, hint);
     elem_out = cur;
 }
 
 }  // namespace
 
-__global__ void __launch_bounds__(128) k_btrack(Dev d, Phys P, VG vg) {
+__global__ void __launch_bounds__(128, 8) k_btrack(Dev d, Phys P, VG vg) {
     const int NS = d.NS, NP = d.NP, NE = d.NE, nvrt = P.nvrt;
     const long long total = (long long)NS * nvrt;
     const int ndelt_max = (int)fmax(1.0, P.dt / P.dtb_min);
     const int ndelt_min = (int)fmax(1.0, P.dt / P.dtb_max);
     const double vm2 = P.velmin * P.velmin;
-    for (long long qi = blockIdx.x * (long long)blockDim.x + threadIdx.x; qi < total;
-         qi += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(qi / NS), s = (int)(qi - (long long)k * NS);
+    if (NS <= 0) return;
+    // query q = k * NS + s, visited with a grid stride; (k, s) carried instead of divided
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long q0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int k = (int)(q0 / NS), s = (int)(q0 - (long long)k * NS);
+    const int dk = (int)(stride / NS), ds = (int)(stride - (long long)dk * NS);
+    for (long long qi = q0; qi < total; qi += stride, k += dk, s += ds) {
+        if (s >= NS) { s -= NS; k++; }
         const double2 u = d.su2[(size_t)k * NS + s];
         double2 bt = u;
         int be = -1;

@@ -56,6 +56,7 @@ struct Prepared {
     std::vector<int32_t> en, es;          // [3][NE]
     std::vector<double> gphi;             // [3][NE][2]
     std::vector<int8_t> ssg;              // [3][NE]
+    std::vector<ElemGeo> egeo;            // [NE]
     std::vector<int2> sell;               // SELL-32 slices
     std::vector<int32_t> sidx;            // SELL entries' columns
 };
@@ -404,6 +405,38 @@ static gs_status prepare_host(gs_ctx* c) {
     }
     B.sn.insert(B.sn.end(), sn2.begin(), sn2.end());
     B.se.insert(B.se.end(), se2.begin(), se2.end());
+    // backtracking records: corners in node order, and the node that starts each side in the
+    // element's orientation (the side's first node when the element is the side's first element)
+    pr->egeo.resize(NE);
+    for (int E = 0; E < NE; E++) {
+        ElemGeo& g = pr->egeo[E];
+        std::memset(&g, 0, sizeof(g));
+        for (int j = 0; j < 3; j++) {
+            const int n = en[(size_t)j * NE + E];
+            g.p[j].x = B.x[n]; g.p[j].y = B.y[n];
+            g.n[j] = n;
+        }
+        g.area = B.area[E];
+        for (int j = 0; j < 3; j++) {
+            const int s = es[(size_t)j * NE + E];
+            const int start = ssg[(size_t)j * NE + E] > 0 ? B.sn[s] : B.sn[(size_t)NS + s];
+            const int c = (start == g.n[0]) ? 0 : (start == g.n[1]) ? 1 : 2;
+            g.perm |= c << (2 * j);
+        }
+        // obtuse-corner flags of the walk predicates: side j and side j+1 (in side order) make an
+        // obtuse angle at their shared corner when their direction vectors point the same way
+        double2 C[3];
+        for (int j = 0; j < 3; j++) C[j] = g.p[(g.perm >> (2 * j)) & 3];
+        double2 sv[3];
+        for (int j = 0; j < 3; j++) {
+            const double2 a = C[j], b = C[(j + 1) % 3];
+            sv[j].x = b.x - a.x; sv[j].y = b.y - a.y;
+        }
+        for (int j = 0; j < 3; j++) {
+            const double2 u = sv[j], w = sv[(j + 1) % 3];
+            if (u.x * w.x + u.y * w.y > 0.0) g.perm |= 1 << (8 + j);
+        }
+    }
 
     // SELL-32 layout of the batch matrix; assembly slots move to their SELL positions
     std::vector<int2>& sell = pr->sell;
@@ -504,6 +537,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     UP(en, en); UP(es, es); UP(area, B.area);
     if (e == cudaSuccess) { e = dalloc(c, d.gphi, 3 * (size_t)NE); if (e == cudaSuccess) e = cudaMemcpyAsync(d.gphi, gphi.data(), gphi.size() * 8, cudaMemcpyHostToDevice, c->own_st); }
     UP(ssgn, ssg); AL(kbe, NE); AL(edry, NE);
+    if (e == cudaSuccess) { e = dalloc(c, d.egeo, NE); if (e == cudaSuccess) e = cudaMemcpyAsync(d.egeo, pr->egeo.data(), pr->egeo.size() * sizeof(ElemGeo), cudaMemcpyHostToDevice, c->own_st); }
     AL(ez, (size_t)nvrt * NE); AL(ew, (size_t)nvrt * NE); AL(Qv, (size_t)nvrt * NE);
     UP(etr, B.etr); AL(prev, (size_t)ntr * nvrt * NE); AL(maxDt, NE); AL(ghat, NE);
     UP(mem_np0, B.mem_np0); UP(mem_ne0, B.mem_ne0); UP(elem_member, B.elem_member);
@@ -931,7 +965,7 @@ extern "C" size_t gs_footprint_bytes(int nvrt, int ntr, int nmem, int64_t np, in
     const double sell = (double)nnz * 1.25 + 32.0 * kMaxDeg;
     double b = 0.0;
     b += (double)np * (91.0 + L * (8 + 8 + 16 + 8 * T) + 20.0 + 88.0 + 4.0 * kIrVectors + 4.0 + 332.0);
-    b += (double)ne * (24.0 + 88.0 + 24.0 + 4.0 + L * (24.0 + 16.0 * T));
+    b += (double)ne * (24.0 + 88.0 + 24.0 + 4.0 + 80.0 + L * (24.0 + 16.0 * T));
     b += (double)ns * (16.0 + 70.0 + 72.0 + 16.0 + L * 52.0);
     b += sell * 16.0 + (double)np / 32.0 * 8.0;
     b += ((double)np / 1024.0 + nmem) * 84.0 + (double)nmem * (16.0 + 72.0 + 40.0 + 8.0 * kVortexParams + 64.0);

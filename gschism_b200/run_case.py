@@ -4,6 +4,12 @@
 
 Used to drive profiler captures of one phase on a chosen size: the elevation solve depends on
 the horizontal mesh only, so `--levels` can shrink the device state without changing it.
+
+    python -m gschism_b200.run_case --n 1000 --steps 12 --time-phase BTRACK --repeat 20
+
+times one phase alone on the state reached after the steps (CUDA events around `--repeat`
+launches after 3 untimed ones).  Only phases that do not modify their own inputs give a
+repeatable figure this way (BTRACK does: it reads velocities and writes only its own output).
 """
 from __future__ import annotations
 
@@ -22,6 +28,8 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--precision", choices=["fp64", "fp32_ir"], default="fp32_ir")
     ap.add_argument("--inner-rtol", type=float, default=0.1)
+    ap.add_argument("--time-phase", default=None, help="phase to time after the steps (e.g. BTRACK)")
+    ap.add_argument("--repeat", type=int, default=20)
     a = ap.parse_args(argv)
     t0 = time.time()
     if a.case == "basin":
@@ -35,6 +43,21 @@ def main(argv=None) -> int:
         m.step(1)
         m.sync()
         print("step", s, m.stats(), flush=True)
+    if a.time_phase:
+        import torch
+        st = torch.cuda.Stream()
+        m.set_stream(st.cuda_stream)
+        for _ in range(3):
+            m.phase(a.time_phase)
+        m.sync()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(st)
+        for _ in range(a.repeat):
+            m.phase(a.time_phase)
+        ev[1].record(st)
+        ev[1].synchronize()
+        print(f"phase {a.time_phase}: {ev[0].elapsed_time(ev[1]) / a.repeat:.3f} ms per launch "
+              f"({a.repeat} launches after {a.steps} steps)", flush=True)
     return 0
 
 
