@@ -92,6 +92,7 @@ struct Dev {
     double2 *su2, *btu;            // [nvrt][NS]
     int32_t *btel;                 // [nvrt][NS]
     double2 *U, *gE1, *gE2;
+    double2 *sgh;                  // [3][NS] a side's terms of the element-averaged ghat
     double *hhat, *chi, *chi2;
     // elements
     int32_t *en, *es;              // [3][NE]

@@ -52,24 +52,49 @@ __global__ void k_elev_bc(Dev d) {
 
 __global__ void k_side_prep(Dev d, Phys P) {
     // computeVerticallyIntegratedVelocity (mdc:4459-4476) and
-    // computeVegetationAndDragParameters (mdc:4615-4725, iveg = 0)
+    // computeVegetationAndDragParameters (mdc:4615-4725, iveg = 0); then, for every side of a wet
+    // element, the side's three terms of computeElemAverageGhat (mdc:6183-6424): its
+    // backtracked-velocity column integral and its stress, drag and Coriolis terms, so that the
+    // element pass adds three stored terms per side instead of integrating both columns of every
+    // side once per adjacent element.  Side-parallel: each level's reads are coalesced.
     const int nvrt = P.nvrt, NS = d.NS;
+    const double dt = P.dt;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < NS; s += gridDim.x * blockDim.x) {
         double2 U = v2(0.0, 0.0);
         double hhat = 0.0, chi = 0.0, chi2 = 0.0;
-        if (!d.sdry[s]) {
-            const int kb = d.kbs[s];
+        const int e0 = d.se[s], e1 = d.se[NS + s];
+        const bool ghat_side = (e0 >= 0 && !d.edry[e0]) || (e1 >= 0 && !d.edry[e1]);
+        const int kb = d.kbs[s];
+        const bool is2d = (kb == nvrt - 2);
+        const bool wet = !d.sdry[s];
+        // one pass over the column: the depth integral of the velocity (wet sides) and of the
+        // backtracked velocity (3-D sides of wet elements) over the same level pairs
+        double2 Ustar = v2(0.0, 0.0);
+        const bool col_u = wet, col_b = ghat_side && !is2d;
+        if (col_u || col_b) {
             double zlo = d.zc[(size_t)kb * NS + s];
-            double2 ulo = d.su2[(size_t)kb * NS + s];
-            for (int k = kb; k < nvrt - 1; k++) {
-                const double zhi = d.zc[(size_t)(k + 1) * NS + s];
-                const double2 uhi = d.su2[(size_t)(k + 1) * NS + s];
-                const double2 uc = (ulo + uhi) * 0.5;
-                U = U + uc * (zhi - zlo);
-                zlo = zhi; ulo = uhi;
+            double2 ulo = col_u ? d.su2[(size_t)kb * NS + s] : v2(0.0, 0.0);
+            double2 blo = col_b ? d.btu[(size_t)kb * NS + s] : v2(0.0, 0.0);
+            for (int k = kb + 1; k < nvrt; k++) {
+                const double zhi = d.zc[(size_t)k * NS + s];
+                if (col_u) {
+                    const double2 uhi = d.su2[(size_t)k * NS + s];
+                    const double2 uc = (ulo + uhi) * 0.5;
+                    U = U + uc * (zhi - zlo);
+                    ulo = uhi;
+                }
+                if (col_b) {
+                    const double2 bhi = d.btu[(size_t)k * NS + s];
+                    const double2 w2 = ((bhi + blo) / 2.0) * (zhi - zlo);
+                    Ustar = Ustar + w2;
+                    blo = bhi;
+                }
+                zlo = zhi;
             }
-            const int a = d.sn[s], b = d.sn[NS + s];
-            const double htot = 0.5 * (d.eta2[a] + d.eta2[b]) + 0.5 * (d.depth[a] + d.depth[b]);
+        }
+        const int a = d.sn[s], b = d.sn[NS + s];
+        const double htot = 0.5 * (d.eta2[a] + d.eta2[b]) + 0.5 * (d.depth[a] + d.depth[b]);
+        if (wet) {
             const double2 bt = d.btu[(size_t)(kb + 1) * NS + s];
             const double vmag1 = sqrt(bt.x * bt.x + bt.y * bt.y);
             const double cd = 0.5 * (d.drag[a] + d.drag[b]);
@@ -84,49 +109,38 @@ __global__ void k_side_prep(Dev d, Phys P) {
             }
         }
         d.U[s] = U; d.hhat[s] = hhat; d.chi[s] = chi; d.chi2[s] = chi2;
+        if (!ghat_side) continue;
+        const double cff1 = is2d ? hhat / htot : 1.0;
+        const double cff2 = is2d ? 0.0 : 1.0;
+        if (is2d) {
+            const double dz = d.zc[(size_t)(nvrt - 1) * NS + s] - d.zc[(size_t)(nvrt - 2) * NS + s];
+            Ustar = Ustar + d.btu[(size_t)(nvrt - 1) * NS + s] * dz;
+        }
+        const double2 tau = (v2(d.tau[2 * a], d.tau[2 * a + 1]) + v2(d.tau[2 * b], d.tau[2 * b + 1])) * 0.5;
+        const double2 ubstar = d.btu[(size_t)(kb + 1) * NS + s];
+        const double cor = d.cori[s];
+        const double2 F = U * cor;
+        const double2 fb = d.su2[(size_t)(kb + 1) * NS + s] * cor;
+        d.sgh[s] = Ustar * cff1;
+        d.sgh[NS + s] = ubstar * (chi * dt * cff2) + tau * (dt * cff1);
+        d.sgh[2 * (size_t)NS + s] = F * (cff1 * dt) - fb * (cff2 * chi * dt * dt);
     }
 }
 
 __global__ void k_ghat(Dev d, Phys P) {
     // computeElemAverageGhat, mdc:6183-6424 (ics = 1, iveg = 0, ibc = 1, no horizontal
-    // viscosity, atmospheric pressure or tidal potential)
-    const int nvrt = P.nvrt, NS = d.NS, NE = d.NE;
-    const double dt = P.dt;
+    // viscosity, atmospheric pressure or tidal potential): per side j of the element, in the
+    // reference's order, g += Ustar_j cff1_j; g -= (drag + stress)_j; g += (Coriolis)_j, with the
+    // side terms made by k_side_prep.
+    const int NS = d.NS, NE = d.NE;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < NE; e += gridDim.x * blockDim.x) {
         double2 g = v2(0.0, 0.0);
         if (!d.edry[e]) {
             for (int j = 0; j < 3; j++) {
                 const int s = d.es[j * NE + e];
-                const int kb = d.kbs[s];
-                const int a = d.sn[s], b = d.sn[NS + s];
-                const double chi = d.chi[s];
-                const double htot = 0.5 * (d.eta2[a] + d.eta2[b]) + 0.5 * (d.depth[a] + d.depth[b]);
-                const bool is2d = (kb == nvrt - 2);
-                const double cff1 = is2d ? d.hhat[s] / htot : 1.0;
-                const double cff2 = is2d ? 0.0 : 1.0;
-                double2 Ustar = v2(0.0, 0.0);
-                if (is2d) {
-                    const double dz = d.zc[(size_t)(nvrt - 1) * NS + s] - d.zc[(size_t)(nvrt - 2) * NS + s];
-                    Ustar = Ustar + d.btu[(size_t)(nvrt - 1) * NS + s] * dz;
-                } else {
-                    double2 blo = d.btu[(size_t)kb * NS + s];
-                    double zlo = d.zc[(size_t)kb * NS + s];
-                    for (int k = kb + 1; k < nvrt; k++) {
-                        const double2 bhi = d.btu[(size_t)k * NS + s];
-                        const double zhi = d.zc[(size_t)k * NS + s];
-                        const double2 w2 = ((bhi + blo) / 2.0) * (zhi - zlo);
-                        Ustar = Ustar + w2;
-                        blo = bhi; zlo = zhi;
-                    }
-                }
-                g = g + Ustar * cff1;
-                const double2 tau = (v2(d.tau[2 * a], d.tau[2 * a + 1]) + v2(d.tau[2 * b], d.tau[2 * b + 1])) * 0.5;
-                const double2 ubstar = d.btu[(size_t)(kb + 1) * NS + s];
-                g = g - (ubstar * (chi * dt * cff2) + tau * (dt * cff1));
-                const double cor = d.cori[s];
-                const double2 F = d.U[s] * cor;
-                const double2 fb = d.su2[(size_t)(kb + 1) * NS + s] * cor;
-                g = g + (F * (cff1 * dt) - fb * (cff2 * chi * dt * dt));
+                g = g + d.sgh[s];
+                g = g - d.sgh[NS + s];
+                g = g + d.sgh[2 * (size_t)NS + s];
             }
             g = g * (1.0 / 3);
         }

@@ -533,7 +533,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     UP(sn, B.sn); UP(se, B.se); UP(len, B.len); UP(snx, B.snx); UP(sny, B.sny); UP(scx, B.scx); UP(scy, B.scy);
     UP(cori, B.cori); AL(kbs, NS); AL(sdry, NS); UP(sbt, B.sbt);
     AL(zc, (size_t)nvrt * NS); AL(Qh, (size_t)nvrt * NS); AL(su2, (size_t)nvrt * NS); AL(btu, (size_t)nvrt * NS);
-    AL(btel, (size_t)nvrt * NS); AL(U, NS); AL(gE1, NS); AL(gE2, NS); AL(hhat, NS); AL(chi, NS); AL(chi2, NS);
+    AL(btel, (size_t)nvrt * NS); AL(U, NS); AL(gE1, NS); AL(gE2, NS); AL(sgh, 3 * (size_t)NS); AL(hhat, NS); AL(chi, NS); AL(chi2, NS);
     UP(en, en); UP(es, es); UP(area, B.area);
     if (e == cudaSuccess) { e = dalloc(c, d.gphi, 3 * (size_t)NE); if (e == cudaSuccess) e = cudaMemcpyAsync(d.gphi, gphi.data(), gphi.size() * 8, cudaMemcpyHostToDevice, c->own_st); }
     UP(ssgn, ssg); AL(kbe, NE); AL(edry, NE);
@@ -966,7 +966,7 @@ extern "C" size_t gs_footprint_bytes(int nvrt, int ntr, int nmem, int64_t np, in
     double b = 0.0;
     b += (double)np * (91.0 + L * (8 + 8 + 16 + 8 * T) + 20.0 + 88.0 + 4.0 * kIrVectors + 4.0 + 332.0);
     b += (double)ne * (24.0 + 88.0 + 24.0 + 4.0 + 80.0 + L * (24.0 + 16.0 * T));
-    b += (double)ns * (16.0 + 70.0 + 72.0 + 16.0 + L * 52.0);
+    b += (double)ns * (16.0 + 70.0 + 72.0 + 16.0 + 48.0 + L * 52.0);
     b += sell * 16.0 + (double)np / 32.0 * 8.0;
     b += ((double)np / 1024.0 + nmem) * 84.0 + (double)nmem * (16.0 + 72.0 + 40.0 + 8.0 * kVortexParams + 64.0);
     b += 256.0 * 1024 * 1024;                   // allocation granularity of ~120 allocations
