@@ -24,7 +24,7 @@ PHASE = dict(BEGIN=0, BTRACK=1, PREPARE=2, ASSEMBLE=3, SOLVE=4, UPDATE_ELEV=5, M
 
 EXPORTS = ["gs_grid_build", "gs_ctx_create", "gs_member_add", "gs_ctx_prepare", "gs_ctx_finalize", "gs_ctx_destroy",
            "gs_last_error", "gs_sync", "gs_set_stream", "gs_step", "gs_phase", "gs_state_get", "gs_state_put", "gs_set_tau",
-           "gs_get_stats", "gs_member_sizes", "gs_jcg_create", "gs_jcg_buffers", "gs_jcg_solve_csr",
+           "gs_get_stats", "gs_tracer_mass", "gs_member_sizes", "gs_jcg_create", "gs_jcg_buffers", "gs_jcg_solve_csr",
            "gs_jcg_check", "gs_jcg_destroy", "gs_jcg_last_error", "gs_jcg_solve_csr_noalloc",
            "gs_set_vortex", "gs_footprint_bytes"]
 
@@ -37,7 +37,7 @@ class GsConfig(ctypes.Structure):
                 ("coricoef", c_double), ("rho0", c_double), ("grav", c_double), ("dramp", c_double),
                 ("ihhat", c_int), ("rtol", c_double), ("maxiter", c_int), ("check_every", c_int),
                 ("precision", c_int), ("ir_inner_rtol", c_double), ("ir_inner_maxiter", c_int),
-                ("device", c_int)]
+                ("device", c_int), ("itr_met", c_int), ("tvd_limiter", c_int), ("dfh0", c_double)]
 
 
 class GsMemberDesc(ctypes.Structure):
@@ -94,6 +94,7 @@ def load(build_if_missing: bool = False):
     L.gs_state_put.argtypes = [c_void_p, I, I, c_void_p, c_size_t]
     L.gs_set_tau.argtypes = [c_void_p, I, PD]
     L.gs_get_stats.argtypes = [c_void_p, I, ctypes.POINTER(GsStats)]
+    L.gs_tracer_mass.argtypes = [c_void_p, I, PD]
     L.gs_member_sizes.argtypes = [c_void_p, I] + [ctypes.POINTER(c_int)] * 4
     L.gs_jcg_create.argtypes = [I, I, I, I, ctypes.POINTER(c_void_p)]
     L.gs_jcg_buffers.argtypes = [c_void_p] + [ctypes.POINTER(c_void_p)] * 5

@@ -1,7 +1,8 @@
 """Build of the gschism_b200 native library (nvcc for sm_100a, in-tree).
 
 Produces gschism_b200/_build/libgschism_b200.so from gschism_b200/csrc.  Per-file flags:
-the backtracking kernels are compiled with -fmad=false (bit-exact walk predicates), and host
+the backtracking and transport kernels are compiled with -fmad=false (bit-exact walk predicates,
+limiter branches rounded like the CPU restatement), and host
 code runs with FMA contraction off so the mesh geometry equals the CPU restatement.
 """
 from __future__ import annotations
@@ -17,7 +18,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "libgschism_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-NO_FMA = {"k_btrack.cu"}
+NO_FMA = {"k_btrack.cu", "k_transport.cu"}
 
 
 def _stale(out, deps):

@@ -50,6 +50,9 @@ class Params:
     rtol: float = 1e-12              # JCG relative tolerance
     maxiter: int = 1500              # JCG iteration cap
     check_every: int = 10            # JCG host/device convergence test period
+    itr_met: int = 1                 # tracer transport: 1 upwind (the reference), 3 TVD
+    tvd_limiter: int = 3             # TVD flux limiter: 0 none, 1 minmod, 2 Osher, 3 van Leer, 4 superbee
+    dfh0: float = 0.0                # constant vertical tracer diffusivity [m^2/s] (implicit)
 
 
 @dataclasses.dataclass
@@ -311,6 +314,48 @@ def basin(seed: int = 2, n: int = 1000, nvrt: int = 30, nz: int = 10, ntr: int =
                 iettype=np.array([3]), amig=np.array([M2_OMEGA, S2_OMEGA]),
                 ff=np.array([1.0, 1.0]), face=np.array([0.0, 0.0]), emo=emo, efa=efa,
                 drag=np.full(npn, 2.5e-3), tau=tw, tr_init=tr, nsteps=nsteps)
+
+
+def transport_stress(seed: int = 4, n: int = 2000, nvrt: int = 40, ntr: int = 5, spacing: float = 250.0,
+                     tau_mag: float = 0.1, limiter: int = 3, dfh0: float = 1e-4, shuffle: bool = True,
+                     nsteps: int = 100, dt: float = 120.0) -> Case:
+    """Transport stress case: n x n lattice at `spacing` (2000 x 2000 nodes over 500 km, as the
+    single-mesh basin), closed boundaries, GRF bathymetry 2..4000 m, nvrt SZ levels, a uniform wind
+    stress of `tau_mag` N/m^2 in a seeded direction, and ntr tracers that each hold a sharp front
+    (tanh across a seeded line, 2 km wide) weakening with depth plus two to four Gaussian blobs
+    (radius 2-8 km).  TVD horizontal transport (`limiter`) with implicit vertical diffusion
+    `dfh0`; with no open boundary the tracer mass changes only through the scheme."""
+    rng = np.random.default_rng(seed)
+    length = spacing * (n - 1)
+    x, y, tri, w, s, e, nn = _lattice(n, n, length, length, 0.2, rng)
+    f = _grf(n, n, length, length, 20e3, rng)
+    depth = 2.0 + (4000.0 - 2.0) * f
+    land = [np.concatenate([s, e[1:], nn[::-1][1:], w[::-1][1:-1]])]
+    if shuffle:
+        x, y, depth, tri, _, land, _ = _permute(rng, x, y, depth, tri, [], land, [])
+    vg = _sz_vgrid(nvrt, max(2, nvrt // 3), 4000.0)
+    npn = x.size
+    z = sz_levels(vg, depth, np.zeros(npn))
+    frac = np.clip(-z / 4000.0, 0.0, 1.0)
+    trs = []
+    for _ in range(ntr):
+        ang = rng.uniform(0.0, 2 * math.pi)
+        cx, cy = rng.uniform(0.2, 0.8, 2) * length
+        front = 0.5 * (1.0 + np.tanh(((x - cx) * math.cos(ang) + (y - cy) * math.sin(ang)) / 2000.0))
+        blobs = np.zeros(npn)
+        for _b in range(int(rng.integers(2, 5))):
+            bx, by = rng.uniform(0.0, 1.0, 2) * length
+            r = rng.uniform(2000.0, 8000.0)
+            blobs += rng.uniform(0.3, 1.0) * np.exp(-0.5 * ((x - bx) ** 2 + (y - by) ** 2) / r ** 2)
+        trs.append(front[None, :] * (1.0 - 0.5 * frac) + blobs[None, :])
+    tr = np.stack(trs, axis=0)
+    ang = rng.uniform(0.0, 2 * math.pi)
+    tau = np.broadcast_to(np.array([math.cos(ang), math.sin(ang)]) * tau_mag / 1025.0, (npn, 2)).copy()
+    return Case(name="transport_stress", seed=seed, x=x, y=y, depth=depth, elnode=tri.astype(np.int32),
+                open_bnd=[], land_bnd=land, vgrid=vg,
+                params=Params(dt=dt, rtol=1e-12, itr_met=3, tvd_limiter=limiter, dfh0=dfh0),
+                iettype=np.zeros(0, dtype=np.int64), amig=np.zeros(0), ff=np.zeros(0), face=np.zeros(0),
+                emo=[], efa=[], drag=np.full(npn, 2.5e-3), tau=tau, tr_init=tr, nsteps=nsteps)
 
 
 def ensemble(n_members: int = 64, seed: int = 3, nmin: int = 20_000, nmax: int = 500_000,

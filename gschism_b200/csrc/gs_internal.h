@@ -23,6 +23,7 @@ constexpr int kMaxLevels = 64;
 constexpr int kMaxBfr = 8;
 constexpr int kMaxDeg = 24;        // max node degree supported by the per-row assembly
 constexpr int kVortexParams = 9;  // x0, y0, heading, speed, vmax, rmax, B, rho_air, enabled
+constexpr int kMassBlocks = 256;    // fixed grid of the tracer mass budget (deterministic sums)
 constexpr int kIrVectors = 10;     // FP32 vectors of the refinement solve: (u, w, s, -) x 2, p, d
 
 // Device error bits (gs_stats.error_flags)
@@ -51,6 +52,8 @@ struct Phys {
     double h_s, h_c, theta_f;
     double dt, thetai, h0, dtb_min, dtb_max, velmin, rmaxvel, dfv0, coricoef, rho0, grav, dramp;
     int ihhat;
+    int tvd, tvd_limiter;          // TVD horizontal transport and its limiter (0 none .. 4 superbee)
+    double dfh0;                   // constant vertical tracer diffusivity (implicit; 0 = none)
 };
 
 // Device state of a batch: members concatenated entity-wise, SFC order inside each member.
@@ -104,6 +107,7 @@ struct Dev {
     uint8_t *edry;
     double *ez, *ew, *Qv;          // [nvrt][NE]
     double *etr, *prev;            // [ntr][nvrt][NE]
+    double *tvds;                  // [ntr][nvrt][NE] TVD inflow sums (allocated with TVD only)
     double *maxDt;
     double2 *ghat;
     // members

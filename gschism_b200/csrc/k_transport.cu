@@ -15,6 +15,17 @@
 // forward-sweep values in etr and the eliminated super-diagonal in prev (both level-major, so a
 // warp's accesses are coalesced), instead of per-thread arrays in local memory.  The tracer count
 // is a template parameter, so per-tracer values stay in registers.
+//
+// TVD (itr_met = 3; the reference has only upwind): flux-limited horizontal advection restated
+// from Casulli & Zanolli (2005).  On a face between the upwind prism U and the downwind prism D
+// the face value is C_U + psi(r)/2 (C_D - C_U), r = S_U / (|Q| (C_U - C_D)), S_U = sum over U's
+// interior inflow faces g of |Q_g| (C_g - C_U).  A sub-step is three passes: the inflow sums of
+// the snapshot, the admissible sub-step (every update coefficient non-negative:
+// dt <= V / sum_in |Q| (1 - psi/2 + sum_out psi/(2r))), and the update
+// C_P += dt/V [sum_in |Q| (1 - psi/2)(C_U - C_P) + sum_out |Q| psi/2 (C_P - C_D)].  Limiter 0
+// (psi = 0) reproduces the upwind scheme bit for bit.  The vertical solve optionally adds a
+// constant diffusivity between prism centres.  This file is compiled with -fmad=false so that
+// the limiter's branches see the same rounding as the FP64 CPU restatement.
 #include "dev_common.cuh"
 #include "kernels.h"
 
@@ -33,6 +44,31 @@ struct TrArgs {
 
 __device__ __forceinline__ double evol(const Dev& d, int e, int k) {
     return d.area[e] * (d.ez[(size_t)(k + 1) * d.NE + e] - d.ez[(size_t)k * d.NE + e]);
+}
+
+// flux limiter psi(r): 0 none, 1 minmod, 2 Osher (beta = 2), 3 van Leer, 4 superbee; 0 for r <= 0,
+// the limit value for r beyond 1e300
+__device__ __forceinline__ double tvd_psi(int lim, double r) {
+    if (!(r > 0.0)) return 0.0;
+    if (!(r < 1.0e300)) return lim == 0 ? 0.0 : (lim == 1 ? 1.0 : 2.0);
+    switch (lim) {
+    case 1: return fmin(r, 1.0);
+    case 2: return fmin(r, 2.0);
+    case 3: return (r + r) / (1.0 + r);
+    case 4: return fmax(fmin(2.0 * r, 1.0), fmin(r, 2.0));
+    default: return 0.0;
+    }
+}
+
+// psi of a face with upwind value cu, downwind value cd, flux magnitude aq and upwind inflow sum
+// su; psir = psi / (2 r) (0 when psi = 0)
+__device__ __forceinline__ double tvd_face(int lim, double su, double aq, double cu, double cd, double& psir) {
+    const double dd = cu - cd;
+    if (dd == 0.0) { psir = 0.0; return 0.0; }
+    const double r = su / (aq * dd);
+    const double psi = tvd_psi(lim, r);
+    psir = (psi > 0.0) ? psi / (2.0 * r) : 0.0;
+    return psi;
 }
 
 // The three sides of element e as the horizontal update needs them (loaded once per element).
@@ -82,6 +118,21 @@ __device__ void vertical_upwind(const Dev& d, const Phys& P, int e, double dt, c
         const double qk = d.Qv[(size_t)k * NE + e], qm = d.Qv[(size_t)(k - 1) * NE + e];
         if (k != nvrt - 1 && qk < 0.0) { const double tmp = dbv * fabs(qk); cupp -= tmp; bdia += tmp; }
         if (k - 1 != kb && qm > 0.0) { const double tmp = dbv * fabs(qm); alow -= tmp; bdia += tmp; }
+        if (P.dfh0 > 0.0) {
+            // diffusion across the interfaces with the prisms above and below, over the distance
+            // between prism centres
+            const double ar = d.area[e];
+            if (k != nvrt - 1) {
+                const double zp = d.ez[(size_t)(k + 1) * NE + e], zm = d.ez[(size_t)(k - 1) * NE + e];
+                const double tmp = dbv * (P.dfh0 * ar / (0.5 * (zp - zm)));
+                cupp -= tmp; bdia += tmp;
+            }
+            if (k - 1 != kb) {
+                const double zp = d.ez[(size_t)k * NE + e], zm = d.ez[(size_t)(k - 2) * NE + e];
+                const double tmp = dbv * (P.dfh0 * ar / (0.5 * (zp - zm)));
+                alow -= tmp; bdia += tmp;
+            }
+        }
         const size_t ix = (size_t)k * NE + e;
         if (k == k0) {
             bet = bdia;
@@ -137,6 +188,83 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
         const int par = sub & 1, nxt = par ^ 1;
         const double* src = par ? d.prev : d.etr;     // the sub-step's snapshot
         double* dst = par ? d.etr : d.prev;
+        if (P.tvd) {
+            const int lim = P.tvd_limiter;
+            // TVD pass 1: inflow sums of the snapshot (interior inflow faces, side order)
+            for (int e = gid; e < NE; e += G) {
+                const int m = d.elem_member[e];
+                if (!(((volatile double*)T.rem)[par * nmem + m] > 0.0) || d.edry[e]) continue;
+                const ElemSides q = elem_sides(d, e);
+                for (int k = d.kbe[e] + 1; k < nvrt; k++) {
+                    const size_t ix = (size_t)k * NE + e;
+                    double own[NTR], su[NTR];
+#pragma unroll
+                    for (int t = 0; t < NTR; t++) { own[t] = src[t * trs + ix]; su[t] = 0.0; }
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        if (k <= q.kbs[j] || !q.nbwet[j]) continue;
+                        const double fq = d.Qh[(size_t)k * NS + q.s[j]];
+                        if (q.sg[j] * fq < 0.0) {
+                            const size_t nx = (size_t)k * NE + q.nb[j];
+#pragma unroll
+                            for (int t = 0; t < NTR; t++) su[t] += fabs(fq) * (src[t * trs + nx] - own[t]);
+                        }
+                    }
+#pragma unroll
+                    for (int t = 0; t < NTR; t++) d.tvds[t * trs + ix] = su[t];
+                }
+            }
+            if (!grid_sync(d.bar, d.err)) return;
+            // TVD pass 2: admissible sub-step per element
+            for (int e = gid; e < NE; e += G) {
+                const int m = d.elem_member[e];
+                if (!(((volatile double*)T.rem)[par * nmem + m] > 0.0) || d.edry[e]) continue;
+                const ElemSides q = elem_sides(d, e);
+                double md = kHuge;
+                for (int k = d.kbe[e] + 1; k < nvrt; k++) {
+                    const size_t ix = (size_t)k * NE + e;
+                    const double vol = evol(d, e, k - 1);
+                    double own[NTR], so[NTR], den[NTR];
+#pragma unroll
+                    for (int t = 0; t < NTR; t++) { own[t] = src[t * trs + ix]; so[t] = 0.0; den[t] = 0.0; }
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        if (k <= q.kbs[j] || !q.nbwet[j]) continue;
+                        const double fq = d.Qh[(size_t)k * NS + q.s[j]];
+                        if (q.sg[j] * fq > 0.0) {
+                            const size_t nx = (size_t)k * NE + q.nb[j];
+#pragma unroll
+                            for (int t = 0; t < NTR; t++) {
+                                double psir;
+                                tvd_face(lim, d.tvds[t * trs + ix], fabs(fq), own[t], src[t * trs + nx], psir);
+                                so[t] += psir;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        if (k <= q.kbs[j] || !q.nbwet[j]) continue;
+                        const double fq = d.Qh[(size_t)k * NS + q.s[j]];
+                        if (q.sg[j] * fq < 0.0) {
+                            const size_t nx = (size_t)k * NE + q.nb[j];
+#pragma unroll
+                            for (int t = 0; t < NTR; t++) {
+                                double psir;
+                                const double psi = tvd_face(lim, d.tvds[t * trs + nx], fabs(fq), src[t * trs + nx], own[t], psir);
+                                den[t] += fabs(fq) * (1.0 - 0.5 * psi + so[t]);
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int t = 0; t < NTR; t++) {
+                        const double pd = (den[t] == 0.0) ? kHuge : vol / den[t] * (1.0 - 1.0e-6);
+                        md = fmin(md, pd);
+                    }
+                }
+                d.maxDt[e] = md;
+                atomicMin(&T.mindt[par * nmem + m], (unsigned long long)__double_as_longlong(md));
+            }
+        } else
         // horizontalAdvectionPrepare (meshdata.cu:6493-6559): inflow and max sub-step per element
         for (int e = gid; e < NE; e += G) {
             const int m = d.elem_member[e];
@@ -197,6 +325,34 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
                     if (k <= q.kbs[j]) continue;
                     const double fq = d.Qh[(size_t)k * NS + q.s[j]];
                     const double sQ = q.sg[j] * fq;
+                    if (P.tvd) {
+                        const int lim = P.tvd_limiter;
+                        const double coef = dbv * fabs(fq);
+                        const size_t nx = (size_t)k * NE + q.nb[j];
+                        if (sQ < 0.0) {
+                            if (q.nbwet[j]) {
+#pragma unroll
+                                for (int t = 0; t < NTR; t++) {
+                                    const double cu = src[t * trs + nx];
+                                    double psir;
+                                    const double psi = tvd_face(lim, d.tvds[t * trs + nx], fabs(fq), cu, own[t], psir);
+                                    adv[t] += coef * (1.0 - 0.5 * psi) * (cu - own[t]);
+                                }
+                            } else if (q.bt[j] == 2) {
+#pragma unroll
+                                for (int t = 0; t < NTR; t++) adv[t] += coef * (adv[t] - own[t]);
+                            }
+                        } else if (sQ > 0.0 && q.nbwet[j]) {
+#pragma unroll
+                            for (int t = 0; t < NTR; t++) {
+                                const double cd = src[t * trs + nx];
+                                double psir;
+                                const double psi = tvd_face(lim, d.tvds[t * trs + ix], fabs(fq), own[t], cd, psir);
+                                adv[t] += coef * (0.5 * psi) * (own[t] - cd);
+                            }
+                        }
+                        continue;
+                    }
                     if (sQ >= 0.0) continue;
                     const double coef = dbv * fabs(fq);
                     if (q.nbwet[j]) {
@@ -230,6 +386,63 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
         const double* res = (T.nsub[m] & 1) ? d.prev : d.etr;
         vertical_upwind<NTR>(d, P, e, T.dt, res, d.etr, d.prev);
     }
+}
+
+// Tracer mass budget of one member (elements [e0, e1)): per tracer, the sum over wet prisms of
+// volume x concentration in FP64 with Neumaier's compensated summation.  Every thread sums its
+// prisms, the block merges its threads in a fixed tree and a final one-thread pass merges the
+// blocks in order: the grid is fixed (kMassBlocks), so the result does not depend on the GPU.
+__device__ __forceinline__ void neumaier_add(double& s, double& c, double v) {
+    const double t = s + v;
+    if (fabs(s) >= fabs(v)) c += (s - t) + v;
+    else c += (v - t) + s;
+    s = t;
+}
+
+__global__ void __launch_bounds__(256) k_tracer_mass(Dev d, int nvrt, int ntr, int e0, int e1, double* part) {
+    __shared__ double sh_s[256], sh_c[256];
+    const int tid = threadIdx.x, NE = d.NE;
+    for (int t = 0; t < ntr; t++) {
+        double s = 0.0, c = 0.0;
+        for (int e = e0 + blockIdx.x * blockDim.x + tid; e < e1; e += gridDim.x * blockDim.x) {
+            if (d.edry[e]) continue;
+            for (int k = d.kbe[e] + 1; k < nvrt; k++)
+                neumaier_add(s, c, evol(d, e, k - 1) * d.etr[((size_t)t * nvrt + k) * NE + e]);
+        }
+        sh_s[tid] = s; sh_c[tid] = c;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (tid < w) {
+                double a = sh_s[tid], ca = sh_c[tid];
+                neumaier_add(a, ca, sh_s[tid + w]);
+                sh_s[tid] = a; sh_c[tid] = ca + sh_c[tid + w];
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            part[((size_t)blockIdx.x * ntr + t) * 2] = sh_s[0];
+            part[((size_t)blockIdx.x * ntr + t) * 2 + 1] = sh_c[0];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_tracer_mass_final(int nblk, int ntr, const double* part, double* out) {
+    const int t = threadIdx.x;
+    if (t >= ntr) return;
+    double s = 0.0, c = 0.0;
+    for (int b = 0; b < nblk; b++) {
+        neumaier_add(s, c, part[((size_t)b * ntr + t) * 2]);
+        c += part[((size_t)b * ntr + t) * 2 + 1];
+    }
+    out[t] = s + c;
+}
+
+cudaError_t launch_tracer_mass(const Dev& d, const Phys& P, int e0, int e1, double* part, double* out,
+                               cudaStream_t st) {
+    k_tracer_mass<<<kMassBlocks, 256, 0, st>>>(d, P.nvrt, P.ntr, e0, e1, part);
+    k_tracer_mass_final<<<1, 32, 0, st>>>(kMassBlocks, P.ntr, part, out);
+    return cudaGetLastError();
 }
 
 template <int NTR>

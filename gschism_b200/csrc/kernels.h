@@ -48,6 +48,9 @@ void launch_momentum(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
 void launch_vvel(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
 // k_transport.cu
 cudaError_t launch_transport(const Dev& d, const Phys& P, double dt, cudaStream_t st, int nsm);
+// per-tracer mass of elements [e0, e1): part holds kMassBlocks * ntr * 2 doubles, out ntr
+cudaError_t launch_tracer_mass(const Dev& d, const Phys& P, int e0, int e1, double* part, double* out,
+                               cudaStream_t st);
 // k_levels.cu
 void launch_geometry(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
 void launch_levels(const Dev& d, const Phys& P, const VG& vg, int it, cudaStream_t st, int nsm);

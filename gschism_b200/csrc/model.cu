@@ -89,6 +89,8 @@ struct gs_ctx {
     std::vector<double> h_vort;
     int nvortex = 0;
     Prepared* prep = nullptr;        // host preparation awaiting gs_ctx_finalize
+    double* mass_part = nullptr;     // tracer mass budget: per-block partials and result
+    double* mass_out = nullptr;
     gs_status fail(gs_status s, const std::string& m) { err = m; return s; }
 };
 
@@ -138,6 +140,9 @@ gs_status gs_ctx_create(const gs_config* cfg, gs_ctx** out) {
     if (!cfg || !out) return GS_ERR_ARG;
     if (cfg->nvrt < 2 || cfg->nvrt > kMaxLevels || cfg->ntr < 0 || cfg->ntr > kMaxTracers || cfg->nz < 1 ||
         cfg->nz > cfg->nvrt)
+        return GS_ERR_ARG;
+    if ((cfg->itr_met != 0 && cfg->itr_met != 1 && cfg->itr_met != 3) || cfg->tvd_limiter < 0 ||
+        cfg->tvd_limiter > 4 || !(cfg->dfh0 >= 0.0))
         return GS_ERR_ARG;
     gs_ctx* c = new gs_ctx();
     c->cfg = *cfg;
@@ -539,12 +544,15 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     UP(ssgn, ssg); AL(kbe, NE); AL(edry, NE);
     if (e == cudaSuccess) { e = dalloc(c, d.egeo, NE); if (e == cudaSuccess) e = cudaMemcpyAsync(d.egeo, pr->egeo.data(), pr->egeo.size() * sizeof(ElemGeo), cudaMemcpyHostToDevice, c->own_st); }
     AL(ez, (size_t)nvrt * NE); AL(ew, (size_t)nvrt * NE); AL(Qv, (size_t)nvrt * NE);
-    UP(etr, B.etr); AL(prev, (size_t)ntr * nvrt * NE); AL(maxDt, NE); AL(ghat, NE);
+    UP(etr, B.etr); AL(prev, (size_t)ntr * nvrt * NE);
+    if (c->cfg.itr_met == 3) AL(tvds, (size_t)ntr * nvrt * NE); AL(maxDt, NE); AL(ghat, NE);
     UP(mem_np0, B.mem_np0); UP(mem_ne0, B.mem_ne0); UP(elem_member, B.elem_member);
     c->h_vort.assign((size_t)kVortexParams * c->mem.size(), 0.0);
     UP(vort, c->h_vort);
     AL(mem_rem, 2 * (size_t)d.nmem); AL(mem_dtb, d.nmem); AL(mem_mindt, 2 * (size_t)d.nmem + 1); AL(mem_nsub, d.nmem);
     AL(clk, 3); AL(bar, 1); AL(err, 1); AL(counters, 4);
+    if (e == cudaSuccess) e = dalloc(c, c->mass_part, (size_t)kMassBlocks * kMaxTracers * 2);
+    if (e == cudaSuccess) e = dalloc(c, c->mass_out, (size_t)kMaxTracers);
 #undef UP
 #undef AL
     if (e != cudaSuccess) return c->fail(e == cudaErrorMemoryAllocation ? GS_ERR_OOM : GS_ERR_CUDA, cudaGetErrorString(e));
@@ -561,6 +569,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     P.dt = g.dt; P.thetai = g.thetai; P.h0 = g.h0; P.dtb_min = g.dtb_min; P.dtb_max = g.dtb_max;
     P.velmin = g.velmin_btrack; P.rmaxvel = g.rmaxvel; P.dfv0 = g.dfv0; P.coricoef = g.coricoef;
     P.rho0 = g.rho0; P.grav = g.grav; P.dramp = g.dramp; P.ihhat = g.ihhat;
+    P.tvd = (g.itr_met == 3); P.tvd_limiter = g.tvd_limiter; P.dfh0 = g.dfh0;
     VG& vg = c->vg;
     std::memset(&vg, 0, sizeof(vg));
     vg.nvrt = nvrt; vg.nz = g.nz; vg.h_s = g.h_s; vg.h_c = g.h_c; vg.h0 = g.h0;
@@ -739,6 +748,18 @@ gs_status gs_get_stats(gs_ctx* c, int member, gs_stats* out) {
     out->btrack_stops = (int64_t)cnt[1];
     out->error_flags = flags;
     return s == GS_OK ? GS_OK : s;
+}
+
+gs_status gs_tracer_mass(gs_ctx* c, int member, double* out) {
+    if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size() || !out) return GS_ERR_ARG;
+    const int ntr = c->cfg.ntr;
+    if (ntr == 0) return GS_OK;
+    const MemberHost& m = c->mem[member];
+    cudaError_t e = launch_tracer_mass(c->d, c->P, m.ne0, m.ne0 + m.ne, c->mass_part, c->mass_out, c->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, c->mass_out, sizeof(double) * ntr, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    return GS_OK;
 }
 
 gs_status gs_ctx_destroy(gs_ctx* c) {
@@ -969,6 +990,7 @@ extern "C" size_t gs_footprint_bytes(int nvrt, int ntr, int nmem, int64_t np, in
     b += (double)ns * (16.0 + 70.0 + 72.0 + 16.0 + 48.0 + L * 52.0);
     b += sell * 16.0 + (double)np / 32.0 * 8.0;
     b += ((double)np / 1024.0 + nmem) * 84.0 + (double)nmem * (16.0 + 72.0 + 40.0 + 8.0 * kVortexParams + 64.0);
+    b += (double)kMassBlocks * kMaxTracers * 16.0 + kMaxTracers * 8.0;
     b += 256.0 * 1024 * 1024;                   // allocation granularity of ~120 allocations
     return (size_t)b;
 }

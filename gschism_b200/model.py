@@ -86,6 +86,7 @@ class Model:
         cfg.precision = {"fp64": L.GS_FP64, "fp32_ir": L.GS_FP32_IR}[precision]
         cfg.ir_inner_rtol, cfg.ir_inner_maxiter = float(ir_inner_rtol), int(ir_inner_maxiter)
         cfg.device = int(device)
+        cfg.itr_met, cfg.tvd_limiter, cfg.dfh0 = int(p.itr_met), int(p.tvd_limiter), float(p.dfh0)
         self.precision = precision
         h = ctypes.c_void_p()
         L.check(self.lib.gs_ctx_create(ctypes.byref(cfg), ctypes.byref(h)), None, "gs_ctx_create")
@@ -167,6 +168,14 @@ class Model:
         s = L.GsStats()
         L.check(self.lib.gs_get_stats(self.h, member, ctypes.byref(s)), self.h, "gs_get_stats")
         return {f: getattr(s, f) for f, _ in L.GsStats._fields_}
+
+    def tracer_mass(self, member: int = 0) -> np.ndarray:
+        """FP64 tracer mass of a member (sum of prism volume x concentration per tracer,
+        compensated, deterministic): gs_tracer_mass."""
+        out = np.zeros(self.ntr, dtype=np.float64)
+        if self.ntr:
+            L.check(self.lib.gs_tracer_mass(self.h, member, _pd(out)), self.h, "gs_tracer_mass")
+        return out
 
     # ----------------------------------------------------------------------------- state
     def shape(self, member: int, name: str):

@@ -72,6 +72,13 @@ typedef struct {
                                               restart the inner CG every sweep. */
     int ir_inner_maxiter;                  /* iteration cap of one sweep (< 1: 200) */
     int device;                            /* CUDA device ordinal */
+    int itr_met;                           /* tracer transport: 1 (or 0) first-order upwind, the
+                                              reference's scheme; 3 TVD (flux-limited horizontal
+                                              advection, Casulli & Zanolli 2005) */
+    int tvd_limiter;                       /* itr_met = 3: 0 none (first order), 1 minmod,
+                                              2 Osher (beta = 2), 3 van Leer, 4 superbee */
+    double dfh0;                           /* constant vertical tracer diffusivity (m^2/s), implicit;
+                                              0 = none (the reference has none) */
 } gs_config;
 
 typedef struct {
@@ -181,6 +188,11 @@ typedef struct {
     int32_t error_flags;       /* device error bits (bounded waits, non-convergence) */
 } gs_stats;
 gs_status gs_get_stats(gs_ctx* ctx, int member, gs_stats* out);
+/* Tracer mass of a member: for each of the ntr tracers, the sum over the member's wet prisms of
+   volume x concentration (out[ntr]), in FP64 with compensated (Neumaier two-sum) accumulation in a
+   fixed order, so the value does not depend on the GPU or the launch.  The reference has no mass
+   budget; this is the FP64 budget the mass-conservation checks read. */
+gs_status gs_tracer_mass(gs_ctx* ctx, int member, double* out);
 /* sizes of a member: np, ne, ns, nnz (CSR of the elevation matrix) */
 gs_status gs_member_sizes(gs_ctx* ctx, int member, int* np, int* ne, int* ns, int* nnz);
 

@@ -111,6 +111,7 @@ og_model* og_model_create(const og_input* in, int* status) {
     m->dtb_max = in->dtb_max; m->velmin = in->velmin_btrack; m->rmaxvel = in->rmaxvel;
     m->dfv0 = in->dfv0; m->coricoef = in->coricoef; m->rho0 = in->rho0; m->grav = in->grav;
     m->dramp = in->dramp; m->ihhat = in->ihhat;
+    m->itr_met = in->itr_met; m->tvd_limiter = in->tvd_limiter; m->dfh0 = in->dfh0;
     m->nz = in->nz; m->h_s = in->h_s; m->h_c = in->h_c; m->theta_b = in->theta_b; m->theta_f = in->theta_f;
     const int np = m->np, ne = m->ne, nvrt = m->nvrt, ntr = m->ntr;
     m->ztot = (double*)xc(nvrt + 1, sizeof(double));
@@ -233,6 +234,7 @@ og_model* og_model_create(const og_input* in, int* status) {
     m->prev = (double*)xc((size_t)ne * nvrt * (ntr ? ntr : 1), 8);
     m->inflow = (double*)xc((size_t)ne * nvrt, 8);
     m->maxDt = (double*)xc(ne, 8);
+    m->tvds = (double*)xc((size_t)ne * nvrt * (ntr ? ntr : 1), 8);
     m->ghat = (v2*)xc(ne, sizeof(v2));
 
     /* CSR pattern */
@@ -257,7 +259,7 @@ void og_model_free(og_model* m) {
                     m->land_start, m->land_nodes, m->len, m->snx, m->sny, m->scx, m->scy, m->cori,
                     m->kbs, m->sdry, m->sbt, m->zc, m->su2, m->btu, m->btel, m->U, m->hhat, m->chi,
                     m->chi2, m->gE1, m->gE2, m->Qh, m->area, m->edepth, m->gphi, m->ssign, m->kbe,
-                    m->edry, m->ez, m->ew, m->Qv, m->etr, m->prev, m->inflow, m->maxDt, m->ghat,
+                    m->edry, m->ez, m->ew, m->Qv, m->etr, m->prev, m->inflow, m->maxDt, m->ghat, m->tvds,
                     m->indptr, m->indices, m->data, m->slot, m->dslot, m->jr, m->jz, m->jp, m->jq,
                     m->jinvD, m->jb};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);

@@ -4,7 +4,9 @@
  * itur = 0 (constant vertical viscosity), no vegetation, no baroclinic force (ibc = 1),
  * nchi = 0 (drag coefficient per node), imm = 0, ihorcon = 0, ntip = 0 (no tidal potential),
  * no atmospheric pressure, open boundaries with iettype 0/3 (none / tidal harmonics) and
- * ifltype = 0, first-order upwind transport (itr_met = 1).
+ * ifltype = 0, first-order upwind transport (itr_met = 1, the reference's scheme) or flux-limited
+ * TVD horizontal transport (itr_met = 3, restated from Casulli & Zanolli 2005: the reference has
+ * no TVD), optional constant vertical tracer diffusivity.
  */
 #ifndef GS_ORACLE_STEP_H
 #define GS_ORACLE_STEP_H
@@ -33,6 +35,8 @@ typedef struct {
     const double* sigma;         /* [nvrt-nz+1] */
     double dt, thetai, h0, dtb_min, dtb_max, velmin_btrack, rmaxvel, dfv0, coricoef, rho0, grav, dramp;
     int ihhat;
+    int itr_met, tvd_limiter;    /* transport: 1 upwind, 3 TVD; limiter 0 none .. 4 superbee */
+    double dfh0;                 /* constant vertical tracer diffusivity (implicit) */
 } og_input;
 
 /* Exchange field codes (level-major [nvrt][n] for per-level fields, components interleaved

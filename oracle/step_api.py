@@ -34,7 +34,8 @@ class OgInput(ctypes.Structure):
                 ("dt", c_double), ("thetai", c_double), ("h0", c_double), ("dtb_min", c_double),
                 ("dtb_max", c_double), ("velmin_btrack", c_double), ("rmaxvel", c_double),
                 ("dfv0", c_double), ("coricoef", c_double), ("rho0", c_double), ("grav", c_double),
-                ("dramp", c_double), ("ihhat", c_int)]
+                ("dramp", c_double), ("ihhat", c_int), ("itr_met", c_int), ("tvd_limiter", c_int),
+                ("dfh0", c_double)]
 
 
 def declare(L) -> None:
@@ -112,6 +113,7 @@ class OracleModel:
                      "coricoef", "rho0", "grav", "dramp"):
             setattr(inp, name, float(getattr(p, name)))
         inp.ihhat = int(p.ihhat)
+        inp.itr_met, inp.tvd_limiter, inp.dfh0 = int(p.itr_met), int(p.tvd_limiter), float(p.dfh0)
         st = c_int(0)
         self.h = self.L.og_model_create(ctypes.byref(inp), ctypes.byref(st))
         if st.value != 0:

@@ -22,6 +22,7 @@ struct og_model {
     int np, ne, ns, nvrt, ntr, nope, nland, nbfr, nnz;
     double dt, thetai, h0, dtb_min, dtb_max, velmin, rmaxvel, dfv0, coricoef, rho0, grav, dramp;
     int ihhat;
+    int itr_met, tvd_limiter; double dfh0;
     double rtol; int maxiter, check_every;
     int nz; double h_s, h_c, theta_b, theta_f;
     double *ztot, *sigma, *cs;
@@ -49,6 +50,7 @@ struct og_model {
     double *area, *edepth; v2* gphi; double* ssign;
     int32_t* kbe; uint8_t* edry;
     double *ez, *ew, *Qv, *etr, *prev, *inflow, *maxDt; v2* ghat;
+    double* tvds;                 /* TVD: inflow sum per prism and tracer [ne][nvrt][ntr] */
     int64_t cnt[4];
 };
 

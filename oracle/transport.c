@@ -2,7 +2,19 @@
  * Restates computeTransport (schism_step.py:78-93): computeHorizAdvecFluxes (mdc:6461-6491),
  * the sub-cycled horizontalAdvectionPrepare / minTransportDt / horizontalAdvectionUpdate
  * (mdc:6493-6609, 6842-6863), verticalAdvectionUpdate (mdc:6611-6665) and nodalTracerUpdate
- * (mdc:6739-6774); first-order upwind (TransportModel::Upwind, mdh:469-483). */
+ * (mdc:6739-6774); first-order upwind (TransportModel::Upwind, mdh:469-483).
+ *
+ * The TVD option (itr_met = 3) has no counterpart in the reference and is restated from the
+ * published scheme (Casulli & Zanolli 2005, as used by SCHISM's TVD transport): on a horizontal
+ * face f between the upwind prism U and the downwind prism D the face value is
+ * C_U + psi(r_f)/2 (C_D - C_U), with r_f = S_U / (|Q_f| (C_U - C_D)) and S_U the sum over U's
+ * interior inflow faces g of |Q_g| (C_g - C_U).  In the non-conservative form of the reference's
+ * upwind update this gives, for prism P,
+ *   C_P' = C_P + dt/V [ sum_in |Q| (1 - psi/2) (C_U - C_P) + sum_out |Q| psi/2 (C_P - C_D) ],
+ * and the sub-step keeps every coefficient non-negative: dt <= V / sum_in |Q| (1 - psi/2 + so)
+ * with so = sum_out psi/(2 r) (the outflow terms rewritten through r), times (1 - 1e-6).  With
+ * limiter 0 (psi = 0) it is the upwind scheme bit for bit.  The vertical solve optionally adds a
+ * constant diffusivity dfh0 between prism centres, implicitly (symmetric, conservative). */
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -27,6 +39,152 @@ static void tridag1(int n, const double* a, const double* b, const double* c, co
     for (int j = n - 2; j >= 0; j--) u[j] = u[j] - gam[j + 1] * u[j + 1];
 }
 
+/* flux limiter psi(r): 0 none, 1 minmod, 2 Osher (beta = 2), 3 van Leer, 4 superbee; every
+ * limiter is 0 for r <= 0, and r beyond 1e300 takes the limit value */
+static double tvd_psi(int lim, double r) {
+    if (!(r > 0.0)) return 0.0;
+    if (!(r < 1.0e300)) return lim == 0 ? 0.0 : (lim == 1 ? 1.0 : 2.0);
+    switch (lim) {
+    case 1: return fmin(r, 1.0);
+    case 2: return fmin(r, 2.0);
+    case 3: return (r + r) / (1.0 + r);
+    case 4: return fmax(fmin(2.0 * r, 1.0), fmin(r, 2.0));
+    default: return 0.0;
+    }
+}
+
+/* psi of a face with upwind value cu, downwind value cd, flux magnitude aq and upwind inflow
+ * sum su; *psir = psi / (2 r) (0 when psi = 0) */
+static double tvd_face(int lim, double su, double aq, double cu, double cd, double* psir) {
+    const double d = cu - cd;
+    if (d == 0.0) { *psir = 0.0; return 0.0; }
+    const double r = su / (aq * d);
+    const double psi = tvd_psi(lim, r);
+    *psir = (psi > 0.0) ? psi / (2.0 * r) : 0.0;
+    return psi;
+}
+
+static inline int face_nb(const og_model* m, int e, int s) {
+    return (m->isdel[2 * s] == e) ? m->isdel[2 * s + 1] : m->isdel[2 * s];
+}
+
+/* one TVD sub-step of the horizontal advection: snapshot, inflow sums, admissible sub-step,
+ * update; returns the sub-step taken */
+static double tvd_substep(og_model* m, double remaining) {
+    const int ne = m->ne, nvrt = m->nvrt, ntr = m->ntr, lim = m->tvd_limiter;
+#define PV(e, k, t) m->prev[((size_t)(e) * nvrt + (k)) * ntr + (t)]
+#define SV(e, k, t) m->tvds[((size_t)(e) * nvrt + (k)) * ntr + (t)]
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < ne; e++) {
+        if (m->edry[e]) continue;
+        memcpy(&m->prev[(size_t)e * nvrt * ntr], &m->etr[(size_t)e * nvrt * ntr], sizeof(double) * nvrt * ntr);
+    }
+    /* S_P: interior inflow faces, in side order */
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < ne; e++) {
+        if (m->edry[e]) continue;
+        for (int k = m->kbe[e] + 1; k < nvrt; k++)
+            for (int t = 0; t < ntr; t++) {
+                double su = 0.0;
+                for (int j = 0; j < 3; j++) {
+                    const int s = m->es[3 * e + j];
+                    if (k <= m->kbs[s]) continue;
+                    const int nb = face_nb(m, e, s);
+                    if (nb < 0 || m->edry[nb]) continue;
+                    const double fq = m->Qh[(size_t)s * nvrt + k];
+                    if (m->ssign[3 * e + j] * fq < 0.0) su += fabs(fq) * (PV(nb, k, t) - PV(e, k, t));
+                }
+                SV(e, k, t) = su;
+            }
+    }
+    /* admissible sub-step per element */
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < ne; e++) {
+        if (m->edry[e]) continue;
+        double md = HUGE_D;
+        for (int k = m->kbe[e] + 1; k < nvrt; k++) {
+            const double vol = evol(m, e, k - 1);
+            for (int t = 0; t < ntr; t++) {
+                double so = 0.0, den = 0.0, psir;
+                for (int j = 0; j < 3; j++) {
+                    const int s = m->es[3 * e + j];
+                    if (k <= m->kbs[s]) continue;
+                    const int nb = face_nb(m, e, s);
+                    if (nb < 0 || m->edry[nb]) continue;
+                    const double fq = m->Qh[(size_t)s * nvrt + k];
+                    if (m->ssign[3 * e + j] * fq > 0.0) {
+                        tvd_face(lim, SV(e, k, t), fabs(fq), PV(e, k, t), PV(nb, k, t), &psir);
+                        so += psir;
+                    }
+                }
+                for (int j = 0; j < 3; j++) {
+                    const int s = m->es[3 * e + j];
+                    if (k <= m->kbs[s]) continue;
+                    const int nb = face_nb(m, e, s);
+                    if (nb < 0 || m->edry[nb]) continue;
+                    const double fq = m->Qh[(size_t)s * nvrt + k];
+                    if (m->ssign[3 * e + j] * fq < 0.0) {
+                        const double psi = tvd_face(lim, SV(nb, k, t), fabs(fq), PV(nb, k, t), PV(e, k, t), &psir);
+                        den += fabs(fq) * (1.0 - 0.5 * psi + so);
+                    }
+                }
+                const double pd = (den == 0.0) ? HUGE_D : vol / den * (1.0 - 1.0e-6);
+                md = fmin(md, pd);
+            }
+        }
+        m->maxDt[e] = md;
+    }
+    double mdt = 1e34;
+    for (int e = 0; e < ne; e++) mdt = fmin(mdt, m->edry[e] ? HUGE_D : m->maxDt[e]);
+    const double dtb = fmin(remaining, mdt);
+    /* update, faces in side order, tracers inner */
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < ne; e++) {
+        if (m->edry[e]) continue;
+        const int kb = m->kbe[e];
+        double* tr = &m->etr[(size_t)e * nvrt * ntr];
+        for (int k = kb + 1; k < nvrt; k++) {
+            const double dbv = dtb / evol(m, e, k - 1);
+            double adv[64];
+            for (int t = 0; t < ntr; t++) adv[t] = PV(e, k, t);
+            for (int j = 0; j < 3; j++) {
+                const int s = m->es[3 * e + j];
+                if (k <= m->kbs[s]) continue;
+                const double fq = m->Qh[(size_t)s * nvrt + k];
+                const double sQ = m->ssign[3 * e + j] * fq;
+                const int nb = face_nb(m, e, s);
+                const int interior = nb >= 0 && !m->edry[nb];
+                const double coef = dbv * fabs(fq);
+                double psir;
+                if (sQ < 0.0) {
+                    if (interior) {
+                        for (int t = 0; t < ntr; t++) {
+                            const double own = PV(e, k, t), cu = PV(nb, k, t);
+                            const double psi = tvd_face(lim, SV(nb, k, t), fabs(fq), cu, own, &psir);
+                            adv[t] += coef * (1.0 - 0.5 * psi) * (cu - own);
+                        }
+                    } else if (m->sbt[s] == 2) {
+                        /* open boundary inflow: Cout keeps the running value (mdc:6585-6592) */
+                        for (int t = 0; t < ntr; t++) adv[t] += coef * (adv[t] - PV(e, k, t));
+                    }
+                } else if (sQ > 0.0 && interior) {
+                    for (int t = 0; t < ntr; t++) {
+                        const double own = PV(e, k, t), cd = PV(nb, k, t);
+                        const double psi = tvd_face(lim, SV(e, k, t), fabs(fq), own, cd, &psir);
+                        adv[t] += coef * (0.5 * psi) * (own - cd);
+                    }
+                }
+            }
+            for (int t = 0; t < ntr; t++) tr[k * ntr + t] = adv[t];
+        }
+        for (int k = 0; k <= kb; k++)
+            for (int t = 0; t < ntr; t++) tr[k * ntr + t] = tr[(kb + 1) * ntr + t];
+    }
+#undef PV
+#undef SV
+    return dtb;
+}
+
 int og_transport(og_model* m, double dt) {
     const int ne = m->ne, ns = m->ns, nvrt = m->nvrt, ntr = m->ntr;
     /* computeHorizAdvecFluxes */
@@ -47,7 +205,11 @@ int og_transport(og_model* m, double dt) {
     }
     double remaining = dt;
     int nsub = 0;
-    while (remaining > 0.0) {
+    while (m->itr_met == 3 && remaining > 0.0) {
+        remaining -= tvd_substep(m, remaining);
+        nsub++;
+    }
+    while (m->itr_met != 3 && remaining > 0.0) {
         /* horizontalAdvectionPrepare */
 #pragma omp parallel for schedule(static)
         for (int e = 0; e < ne; e++) {
@@ -142,6 +304,19 @@ int og_transport(og_model* m, double dt) {
                 if (k - 1 != kb && Qv[k - 1] > 0.0) {
                     const double tmp = dbv * fabs(Qv[k - 1]);
                     alow[kin] -= tmp; bdia[kin] += tmp;
+                }
+                if (m->dfh0 > 0.0) {
+                    /* diffusion across the interfaces with the prisms above and below, over the
+                       distance between prism centres */
+                    const double* z = &m->ez[(size_t)e * nvrt];
+                    if (k != nvrt - 1) {
+                        const double tmp = dbv * (m->dfh0 * m->area[e] / (0.5 * (z[k + 1] - z[k - 1])));
+                        cupp[kin] -= tmp; bdia[kin] += tmp;
+                    }
+                    if (k - 1 != kb) {
+                        const double tmp = dbv * (m->dfh0 * m->area[e] / (0.5 * (z[k] - z[k - 2])));
+                        alow[kin] -= tmp; bdia[kin] += tmp;
+                    }
                 }
             }
             tridag1(nEq, alow, bdia, cupp, rrhs, soln, gam);
