@@ -19,12 +19,15 @@ GS_FP64, GS_FP32_IR = 0, 1
 STATUS_NAMES = {0: "GS_OK", 1: "GS_ERR_ARG", 2: "GS_ERR_CUDA", 3: "GS_ERR_OOM", 4: "GS_ERR_NOT_CONVERGED",
                 5: "GS_ERR_TIMEOUT", 6: "GS_ERR_BAD_MESH", 7: "GS_ERR_STATE"}
 
+# launch-shape ids of gs_set_launch / gs_get_launch
+LAUNCH = dict(BTRACK=0, SIDE_PREP=1, GHAT=2, ASSEMBLE=3, MOMENTUM=4, VVEL=5, NODAL_VEL=6, NODAL_TRACER=7,
+              LEVELS=8, JCG_TILES=9)
 PHASE = dict(BEGIN=0, BTRACK=1, PREPARE=2, ASSEMBLE=3, SOLVE=4, UPDATE_ELEV=5, MOMENTUM=6, VVEL=7,
              TRANSPORT=8, LEVELS=9, NODAL_VEL=10)
 
 EXPORTS = ["gs_grid_build", "gs_ctx_create", "gs_member_add", "gs_ctx_prepare", "gs_ctx_finalize", "gs_ctx_destroy",
            "gs_last_error", "gs_sync", "gs_set_stream", "gs_step", "gs_phase", "gs_state_get", "gs_state_put", "gs_set_tau",
-           "gs_get_stats", "gs_tracer_mass", "gs_member_sizes", "gs_jcg_create", "gs_jcg_buffers", "gs_jcg_solve_csr",
+           "gs_get_stats", "gs_tracer_mass", "gs_set_launch", "gs_get_launch", "gs_member_sizes", "gs_jcg_create", "gs_jcg_buffers", "gs_jcg_solve_csr",
            "gs_jcg_check", "gs_jcg_destroy", "gs_jcg_last_error", "gs_jcg_solve_csr_noalloc",
            "gs_set_vortex", "gs_footprint_bytes"]
 
@@ -95,6 +98,8 @@ def load(build_if_missing: bool = False):
     L.gs_set_tau.argtypes = [c_void_p, I, PD]
     L.gs_get_stats.argtypes = [c_void_p, I, ctypes.POINTER(GsStats)]
     L.gs_tracer_mass.argtypes = [c_void_p, I, PD]
+    L.gs_set_launch.argtypes = [c_void_p, I, I, I]
+    L.gs_get_launch.argtypes = [c_void_p, I, PI, PI]
     L.gs_member_sizes.argtypes = [c_void_p, I] + [ctypes.POINTER(c_int)] * 4
     L.gs_jcg_create.argtypes = [I, I, I, I, ctypes.POINTER(c_void_p)]
     L.gs_jcg_buffers.argtypes = [c_void_p] + [ctypes.POINTER(c_void_p)] * 5

@@ -106,5 +106,12 @@ inline int grid_for(int n, int block, int max_blocks) {
     if (g > max_blocks) g = max_blocks;
     return g < 1 ? 1 : g;
 }
+// grid of a stream kernel with launch shape s over n entities
+inline int grid_of(long long n, const LaunchShape& s, int nsm) {
+    long long g = (n + s.block - 1) / s.block;
+    const long long cap = (long long)nsm * s.per_sm;
+    if (g > cap) g = cap;
+    return g < 1 ? 1 : (int)g;
+}
 
 }  // namespace gs

@@ -46,6 +46,26 @@ struct alignas(16) ElemGeo {
 };
 static_assert(sizeof(ElemGeo) == 80, "ElemGeo layout");
 
+// Launch shapes of the step's stream kernels: threads per block and the grid cap in blocks per
+// SM (the kernels loop over their entities with a grid stride, so any shape gives the same
+// results), and the tiling of the JCG work list.  The defaults are hand-chosen; gs_set_launch
+// (the autotuner) replaces them.  The kernel ids equal the GS_K_* codes of the C ABI.
+enum : int {
+    LK_BTRACK = 0, LK_SIDE_PREP, LK_GHAT, LK_ASSEMBLE, LK_MOMENTUM, LK_VVEL, LK_NODAL_VEL,
+    LK_NODAL_TRACER, LK_LEVELS, LK_COUNT
+};
+struct LaunchShape { int block, per_sm; };
+struct JcgTiling {
+    int tiles = 592;        // tiles of a large member (one per block of a 4-blocks-per-SM grid)
+    int min_rows = 1024;    // smallest tile (four rows per thread of a 256-thread block)
+    int per_sm = 4;         // cap of the cooperative grid in blocks per SM
+};
+struct LaunchTable {
+    LaunchShape k[LK_COUNT] = {{128, 32}, {256, 16}, {256, 16}, {128, 16}, {128, 32},
+                               {128, 32}, {128, 16}, {128, 16}, {256, 16}};
+    JcgTiling jcg;
+};
+
 // Batch-wide constants shared by all members (copied into kernel arguments).
 struct Phys {
     int nvrt, ntr, nz;

@@ -742,16 +742,15 @@ struct JcgWork {
     unsigned* ndone = nullptr;
 };
 
-// Tile rows of a member: a function of the member's own size only (batch independence).  A
-// large member is cut into about kMemberTiles tiles, i.e. one per block of a 4-blocks-per-SM grid
-// on a 148-SM part, so its rows spread evenly over the SMs.  Tiles never go below kMinTileRows
-// (four rows per thread): every tile ends in a block-wide reduction, and smaller tiles leave too
-// little independent work between those reductions.
-constexpr int kMemberTiles = 592;
-constexpr int kMinTileRows = 1024;
-static int tile_rows_for(int rows) {
-    const long long per = ((long long)rows + kMemberTiles - 1) / kMemberTiles;
-    return (int)std::max((long long)kMinTileRows, (per + 31) / 32 * 32);
+// Tile rows of a member: a function of the member's own size and the tiling only (batch
+// independence).  By default a large member is cut into about 592 tiles, i.e. one per block of a
+// 4-blocks-per-SM grid on a 148-SM part, so its rows spread evenly over the SMs, and tiles never
+// go below 1,024 rows (four rows per thread): every tile ends in a block-wide reduction, and
+// smaller tiles leave too little independent work between those reductions.  The autotuner may
+// choose other values (JcgTiling).
+static int tile_rows_for(int rows, const JcgTiling& tl) {
+    const long long per = ((long long)rows + tl.tiles - 1) / tl.tiles;
+    return (int)std::max((long long)tl.min_rows, (per + 31) / 32 * 32);
 }
 
 // Contiguous tile ranges per block with about the same number of rows in each.
@@ -770,21 +769,21 @@ static void block_ranges(const std::vector<int32_t>& tr0, const std::vector<int3
     }
 }
 
-static int coop_blocks(const void* fn, int nsm) {
+static int coop_blocks(const void* fn, int nsm, int cap = 4) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0);
     if (per_sm < 1) per_sm = 1;
-    if (per_sm > 4) per_sm = 4;
+    if (per_sm > cap) per_sm = cap;
     return nsm * per_sm;
 }
 
 cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std::vector<int>& rows, bool sell,
-                           cudaStream_t st) {
+                           cudaStream_t st, const JcgTiling& tiling) {
     w = new JcgWork();
     const int nmem = (int)rows.size();
     std::vector<int32_t> tr0, tr1, tm, mt0(nmem), mt1(nmem);
     for (int m = 0; m < nmem; m++) {
-        const int tr = tile_rows_for(rows[m]);
+        const int tr = tile_rows_for(rows[m], tiling);
         mt0[m] = (int)tr0.size();
         for (int r = 0; r < rows[m]; r += tr) {
             tr0.push_back(row0[m] + r);
@@ -802,8 +801,8 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     const void* f64 = sell ? (const void*)k_jcg64<true> : (const void*)k_jcg64<false>;
     const void* fir = sell ? (const void*)k_jcg_ir<true> : (const void*)k_jcg_ir<false>;
     w->sell = sell;
-    w->grid64 = std::max(1, std::min(T, coop_blocks(f64, nsm)));
-    w->gridir = std::max(1, std::min(T, coop_blocks(fir, nsm)));
+    w->grid64 = std::max(1, std::min(T, coop_blocks(f64, nsm, tiling.per_sm)));
+    w->gridir = std::max(1, std::min(T, coop_blocks(fir, nsm, tiling.per_sm)));
     std::vector<int32_t> b64, bir;
     block_ranges(tr0, tr1, w->grid64, b64);
     block_ranges(tr0, tr1, w->gridir, bir);

@@ -271,12 +271,15 @@ __global__ void __launch_bounds__(128, 8) k_btrack(Dev d, Phys P, VG vg) {
     }
 }
 
-void launch_btrack(const Dev& d, const Phys& P, const VG& vg, cudaStream_t st, int nsm) {
+void launch_btrack(const Dev& d, const Phys& P, const VG& vg, cudaStream_t st, int nsm, const LaunchTable& L) {
     cudaMemsetAsync(d.counters, 0, 2 * sizeof(unsigned long long), st);
-    const long long total = (long long)d.NS * P.nvrt;
-    int grid = (int)std::min<long long>((total + 127) / 128, (long long)nsm * 32);
-    if (grid < 1) grid = 1;
-    k_btrack<<<grid, 128, 0, st>>>(d, P, vg);
+    const LaunchShape& s = L.k[LK_BTRACK];
+    k_btrack<<<grid_of((long long)d.NS * P.nvrt, s, nsm), s.block, 0, st>>>(d, P, vg);
+}
+
+int btrack_max_threads() {
+    cudaFuncAttributes a{};
+    return cudaFuncGetAttributes(&a, k_btrack) == cudaSuccess ? a.maxThreadsPerBlock : 0;
 }
 
 }  // namespace gs

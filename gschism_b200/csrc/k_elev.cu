@@ -288,15 +288,26 @@ __global__ void k_vortex_tau(Dev d, double rho0) {
 void launch_clock_set(const Dev& d, const Phys& P, int it, cudaStream_t st) { k_clock_set<<<1, 1, 0, st>>>(d, P, it); }
 void launch_clock_advance(const Dev& d, const Phys& P, cudaStream_t st) { k_clock_advance<<<1, 1, 0, st>>>(d, P); }
 
-void launch_elev_prepare(const Dev& d, const Phys& P, bool vortex, cudaStream_t st, int nsm) {
+void launch_elev_prepare(const Dev& d, const Phys& P, bool vortex, cudaStream_t st, int nsm, const LaunchTable& L) {
     if (vortex) k_vortex_tau<<<grid_for(d.NP, 256, nsm * 8), 256, 0, st>>>(d, P.rho0);
     if (d.NB > 0) k_elev_bc<<<grid_for(d.NB, 128, nsm * 4), 128, 0, st>>>(d);
-    k_side_prep<<<grid_for(d.NS, 256, nsm * 16), 256, 0, st>>>(d, P);
-    k_ghat<<<grid_for(d.NE, 256, nsm * 16), 256, 0, st>>>(d, P);
+    const LaunchShape &sp = L.k[LK_SIDE_PREP], &gh = L.k[LK_GHAT];
+    k_side_prep<<<grid_of(d.NS, sp, nsm), sp.block, 0, st>>>(d, P);
+    k_ghat<<<grid_of(d.NE, gh, nsm), gh.block, 0, st>>>(d, P);
 }
 
-void launch_assemble(const Dev& d, const Phys& P, cudaStream_t st, int nsm) {
-    k_assemble<<<grid_for(d.NP, 128, nsm * 16), 128, 0, st>>>(d, P);
+void launch_assemble(const Dev& d, const Phys& P, cudaStream_t st, int nsm, const LaunchTable& L) {
+    const LaunchShape& s = L.k[LK_ASSEMBLE];
+    k_assemble<<<grid_of(d.NP, s, nsm), s.block, 0, st>>>(d, P);
+}
+
+int elev_max_threads(int kernel) {
+    cudaFuncAttributes a{};
+    cudaError_t e = cudaErrorInvalidValue;
+    if (kernel == LK_SIDE_PREP) e = cudaFuncGetAttributes(&a, k_side_prep);
+    else if (kernel == LK_GHAT) e = cudaFuncGetAttributes(&a, k_ghat);
+    else if (kernel == LK_ASSEMBLE) e = cudaFuncGetAttributes(&a, k_assemble);
+    return e == cudaSuccess ? a.maxThreadsPerBlock : 0;
 }
 
 void launch_update_elev(const Dev& d, const VG& vg, cudaStream_t st, int nsm) {

@@ -167,17 +167,35 @@ __global__ void k_nodal_vel(Dev d, Phys P) {
     }
 }
 
-void launch_levels(const Dev& d, const Phys& P, const VG& vg, int it, cudaStream_t st, int nsm) {
-    k_lev_nodes<<<grid_for(d.NP, 256, nsm * 16), 256, 0, st>>>(d, vg);
-    k_lev_elems<<<grid_for(d.NE, 256, nsm * 16), 256, 0, st>>>(d, P);
-    k_lev_nodes_dry<<<grid_for(d.NP, 256, nsm * 16), 256, 0, st>>>(d);
-    if (it != 0) k_lev_rewet_nodes<<<grid_for(d.NP, 256, nsm * 16), 256, 0, st>>>(d, P);
-    k_lev_sides<<<grid_for(d.NS, 256, nsm * 16), 256, 0, st>>>(d, P, it);
-    k_lev_sides_dry<<<grid_for(d.NS, 256, nsm * 16), 256, 0, st>>>(d);
+void launch_levels(const Dev& d, const Phys& P, const VG& vg, int it, cudaStream_t st, int nsm, const LaunchTable& L) {
+    const LaunchShape& s = L.k[LK_LEVELS];
+    const int b = s.block;
+    k_lev_nodes<<<grid_of(d.NP, s, nsm), b, 0, st>>>(d, vg);
+    k_lev_elems<<<grid_of(d.NE, s, nsm), b, 0, st>>>(d, P);
+    k_lev_nodes_dry<<<grid_of(d.NP, s, nsm), b, 0, st>>>(d);
+    if (it != 0) k_lev_rewet_nodes<<<grid_of(d.NP, s, nsm), b, 0, st>>>(d, P);
+    k_lev_sides<<<grid_of(d.NS, s, nsm), b, 0, st>>>(d, P, it);
+    k_lev_sides_dry<<<grid_of(d.NS, s, nsm), b, 0, st>>>(d);
 }
 
-void launch_nodal_vel(const Dev& d, const Phys& P, cudaStream_t st, int nsm) {
-    k_nodal_vel<<<grid_for(d.NP, 128, nsm * 16), 128, 0, st>>>(d, P);
+void launch_nodal_vel(const Dev& d, const Phys& P, cudaStream_t st, int nsm, const LaunchTable& L) {
+    const LaunchShape& s = L.k[LK_NODAL_VEL];
+    k_nodal_vel<<<grid_of(d.NP, s, nsm), s.block, 0, st>>>(d, P);
+}
+
+int levels_max_threads(int kernel) {
+    cudaFuncAttributes a{};
+    if (kernel == LK_NODAL_VEL)
+        return cudaFuncGetAttributes(&a, k_nodal_vel) == cudaSuccess ? a.maxThreadsPerBlock : 0;
+    if (kernel != LK_LEVELS) return 0;
+    const void* fs[] = {(const void*)k_lev_nodes, (const void*)k_lev_elems, (const void*)k_lev_nodes_dry,
+                        (const void*)k_lev_rewet_nodes, (const void*)k_lev_sides, (const void*)k_lev_sides_dry};
+    int m = 1024;
+    for (const void* f : fs) {
+        if (cudaFuncGetAttributes(&a, f) != cudaSuccess) return 0;
+        m = std::min(m, a.maxThreadsPerBlock);
+    }
+    return m;
 }
 
 }  // namespace gs

@@ -251,12 +251,22 @@ __global__ void __launch_bounds__(128) k_vvel(Dev d, Phys P) {
     }
 }
 
-void launch_momentum(const Dev& d, const Phys& P, cudaStream_t st, int nsm) {
-    k_momentum<<<grid_for(d.NS, 128, nsm * 32), 128, 0, st>>>(d, P);
+void launch_momentum(const Dev& d, const Phys& P, cudaStream_t st, int nsm, const LaunchTable& L) {
+    const LaunchShape& s = L.k[LK_MOMENTUM];
+    k_momentum<<<grid_of(d.NS, s, nsm), s.block, 0, st>>>(d, P);
 }
 
-void launch_vvel(const Dev& d, const Phys& P, cudaStream_t st, int nsm) {
-    k_vvel<<<grid_for(d.NE, 128, nsm * 32), 128, 0, st>>>(d, P);
+void launch_vvel(const Dev& d, const Phys& P, cudaStream_t st, int nsm, const LaunchTable& L) {
+    const LaunchShape& s = L.k[LK_VVEL];
+    k_vvel<<<grid_of(d.NE, s, nsm), s.block, 0, st>>>(d, P);
+}
+
+int mom_max_threads(int kernel) {
+    cudaFuncAttributes a{};
+    cudaError_t e = cudaErrorInvalidValue;
+    if (kernel == LK_MOMENTUM) e = cudaFuncGetAttributes(&a, k_momentum);
+    else if (kernel == LK_VVEL) e = cudaFuncGetAttributes(&a, k_vvel);
+    return e == cudaSuccess ? a.maxThreadsPerBlock : 0;
 }
 
 }  // namespace gs

@@ -488,7 +488,7 @@ __global__ void k_nodal_tracer(Dev d, Phys P) {
 }
 
 template <int NTR>
-static cudaError_t launch_ntr(const Dev& d, const Phys& P, TrArgs& T, cudaStream_t st, int nsm) {
+static cudaError_t launch_ntr(const Dev& d, const Phys& P, TrArgs& T, cudaStream_t st, int nsm, const LaunchShape& nt) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_transport<NTR>, 256, 0);
     if (per_sm < 1) per_sm = 1;
@@ -500,25 +500,44 @@ static cudaError_t launch_ntr(const Dev& d, const Phys& P, TrArgs& T, cudaStream
     void* args[] = {&dd, &pp, &T};
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_transport<NTR>, dim3(grid), dim3(256), args, 0, st);
     if (e != cudaSuccess) return e;
-    k_nodal_tracer<NTR><<<grid_for(d.NP, 128, nsm * 16), 128, 0, st>>>(d, P);
+    k_nodal_tracer<NTR><<<grid_of(d.NP, nt, nsm), nt.block, 0, st>>>(d, P);
     return cudaGetLastError();
 }
 
-cudaError_t launch_transport(const Dev& d, const Phys& P, double dt, cudaStream_t st, int nsm) {
+template <int NTR>
+static int nodal_tracer_max_threads() {
+    cudaFuncAttributes a{};
+    return cudaFuncGetAttributes(&a, k_nodal_tracer<NTR>) == cudaSuccess ? a.maxThreadsPerBlock : 0;
+}
+
+int transport_max_threads(int ntr) {
+    switch (ntr) {
+    case 1: return nodal_tracer_max_threads<1>();
+    case 2: return nodal_tracer_max_threads<2>();
+    case 3: return nodal_tracer_max_threads<3>();
+    case 4: return nodal_tracer_max_threads<4>();
+    case 5: return nodal_tracer_max_threads<5>();
+    case 6: return nodal_tracer_max_threads<6>();
+    case 7: return nodal_tracer_max_threads<7>();
+    default: return nodal_tracer_max_threads<8>();
+    }
+}
+
+cudaError_t launch_transport(const Dev& d, const Phys& P, double dt, cudaStream_t st, int nsm, const LaunchTable& L) {
     if (P.ntr <= 0) return cudaSuccess;
     TrArgs T;
     T.rem = d.mem_rem; T.mindt = d.mem_mindt; T.nsub = d.mem_nsub; T.active = (unsigned*)(d.mem_mindt + 2 * d.nmem);
     T.dt = dt; T.maxsub = 100000;
     static_assert(kMaxTracers == 8, "one instantiation per tracer count");
     switch (P.ntr) {
-    case 1: return launch_ntr<1>(d, P, T, st, nsm);
-    case 2: return launch_ntr<2>(d, P, T, st, nsm);
-    case 3: return launch_ntr<3>(d, P, T, st, nsm);
-    case 4: return launch_ntr<4>(d, P, T, st, nsm);
-    case 5: return launch_ntr<5>(d, P, T, st, nsm);
-    case 6: return launch_ntr<6>(d, P, T, st, nsm);
-    case 7: return launch_ntr<7>(d, P, T, st, nsm);
-    default: return launch_ntr<8>(d, P, T, st, nsm);
+    case 1: return launch_ntr<1>(d, P, T, st, nsm, L.k[LK_NODAL_TRACER]);
+    case 2: return launch_ntr<2>(d, P, T, st, nsm, L.k[LK_NODAL_TRACER]);
+    case 3: return launch_ntr<3>(d, P, T, st, nsm, L.k[LK_NODAL_TRACER]);
+    case 4: return launch_ntr<4>(d, P, T, st, nsm, L.k[LK_NODAL_TRACER]);
+    case 5: return launch_ntr<5>(d, P, T, st, nsm, L.k[LK_NODAL_TRACER]);
+    case 6: return launch_ntr<6>(d, P, T, st, nsm, L.k[LK_NODAL_TRACER]);
+    case 7: return launch_ntr<7>(d, P, T, st, nsm, L.k[LK_NODAL_TRACER]);
+    default: return launch_ntr<8>(d, P, T, st, nsm, L.k[LK_NODAL_TRACER]);
     }
 }
 

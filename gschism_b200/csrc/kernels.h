@@ -29,7 +29,7 @@ struct JcgArgs {
 };
 struct JcgWork;
 cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std::vector<int>& rows, bool sell,
-                           cudaStream_t st);
+                           cudaStream_t st, const JcgTiling& tiling = JcgTiling());
 void jcg_work_free(JcgWork* w);
 cudaError_t jcg_launch(const JcgArgs& a, JcgWork* w, cudaStream_t st, int nsm);
 cudaError_t jcg_read_iters(JcgWork* w, std::vector<int>& iters, std::vector<int>& outer, cudaStream_t st);
@@ -38,22 +38,28 @@ int32_t* jcg_iters_device(JcgWork* w);
 // k_elev.cu
 void launch_clock_set(const Dev& d, const Phys& P, int it, cudaStream_t st);
 void launch_clock_advance(const Dev& d, const Phys& P, cudaStream_t st);
-void launch_elev_prepare(const Dev& d, const Phys& P, bool vortex, cudaStream_t st, int nsm);
-void launch_assemble(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
+void launch_elev_prepare(const Dev& d, const Phys& P, bool vortex, cudaStream_t st, int nsm, const LaunchTable& L);
+void launch_assemble(const Dev& d, const Phys& P, cudaStream_t st, int nsm, const LaunchTable& L);
 void launch_update_elev(const Dev& d, const VG& vg, cudaStream_t st, int nsm);
 // k_btrack.cu
-void launch_btrack(const Dev& d, const Phys& P, const VG& vg, cudaStream_t st, int nsm);
+void launch_btrack(const Dev& d, const Phys& P, const VG& vg, cudaStream_t st, int nsm, const LaunchTable& L);
 // k_mom.cu
-void launch_momentum(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
-void launch_vvel(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
+void launch_momentum(const Dev& d, const Phys& P, cudaStream_t st, int nsm, const LaunchTable& L);
+void launch_vvel(const Dev& d, const Phys& P, cudaStream_t st, int nsm, const LaunchTable& L);
 // k_transport.cu
-cudaError_t launch_transport(const Dev& d, const Phys& P, double dt, cudaStream_t st, int nsm);
+cudaError_t launch_transport(const Dev& d, const Phys& P, double dt, cudaStream_t st, int nsm, const LaunchTable& L);
 // per-tracer mass of elements [e0, e1): part holds kMassBlocks * ntr * 2 doubles, out ntr
 cudaError_t launch_tracer_mass(const Dev& d, const Phys& P, int e0, int e1, double* part, double* out,
                                cudaStream_t st);
 // k_levels.cu
 void launch_geometry(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
-void launch_levels(const Dev& d, const Phys& P, const VG& vg, int it, cudaStream_t st, int nsm);
-void launch_nodal_vel(const Dev& d, const Phys& P, cudaStream_t st, int nsm);
+void launch_levels(const Dev& d, const Phys& P, const VG& vg, int it, cudaStream_t st, int nsm, const LaunchTable& L);
+void launch_nodal_vel(const Dev& d, const Phys& P, cudaStream_t st, int nsm, const LaunchTable& L);
+// largest block each stream kernel of the launch table can run with (its compiled limits)
+int btrack_max_threads();
+int elev_max_threads(int kernel);
+int mom_max_threads(int kernel);
+int levels_max_threads(int kernel);
+int transport_max_threads(int ntr);
 
 }  // namespace gs

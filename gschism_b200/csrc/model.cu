@@ -89,6 +89,7 @@ struct gs_ctx {
     std::vector<double> h_vort;
     int nvortex = 0;
     Prepared* prep = nullptr;        // host preparation awaiting gs_ctx_finalize
+    LaunchTable launch;              // launch shapes (defaults or the autotuner's)
     double* mass_part = nullptr;     // tracer mass budget: per-block partials and result
     double* mass_out = nullptr;
     gs_status fail(gs_status s, const std::string& m) { err = m; return s; }
@@ -559,7 +560,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     {
         std::vector<int> row0, rows;
         for (auto& m : c->mem) { row0.push_back(m.np0); rows.push_back(m.np); }
-        e = jcg_work_alloc(c->jw, row0, rows, true, c->own_st);
+        e = jcg_work_alloc(c->jw, row0, rows, true, c->own_st, c->launch.jcg);
         if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
     }
     // constants
@@ -581,7 +582,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
                    tb * (std::tanh(tf * (s + 0.5)) - std::tanh(tf * 0.5)) / 2.0 / std::tanh(tf * 0.5);
     }
     // cold start levels (schism_init.py:81-91)
-    launch_levels(c->d, c->P, c->vg, 0, c->st, c->nsm);
+    launch_levels(c->d, c->P, c->vg, 0, c->st, c->nsm, c->launch);
     e = cudaStreamSynchronize(c->st);
     if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
     c->finalized = true;
@@ -595,10 +596,10 @@ static gs_status run_phase(gs_ctx* c, int phase, int arg) {
     cudaStream_t st = c->st;
     switch (phase) {
     case GS_PHASE_BEGIN: c->it = arg; launch_clock_set(c->d, c->P, arg, st); break;
-    case GS_PHASE_BTRACK: launch_btrack(c->d, c->P, c->vg, st, nsm); break;
-    case GS_PHASE_PREPARE: launch_elev_prepare(c->d, c->P, c->nvortex > 0, st, nsm); break;
+    case GS_PHASE_BTRACK: launch_btrack(c->d, c->P, c->vg, st, nsm, c->launch); break;
+    case GS_PHASE_PREPARE: launch_elev_prepare(c->d, c->P, c->nvortex > 0, st, nsm, c->launch); break;
     case GS_PHASE_ASSEMBLE:
-        launch_assemble(c->d, c->P, st, nsm);
+        launch_assemble(c->d, c->P, st, nsm, c->launch);
         break;
     case GS_PHASE_SOLVE: {
         JcgArgs a{};
@@ -615,15 +616,15 @@ static gs_status run_phase(gs_ctx* c, int phase, int arg) {
         break;
     }
     case GS_PHASE_UPDATE_ELEV: launch_update_elev(c->d, c->vg, st, nsm); break;
-    case GS_PHASE_MOMENTUM: launch_momentum(c->d, c->P, st, nsm); break;
-    case GS_PHASE_VVEL: launch_vvel(c->d, c->P, st, nsm); break;
+    case GS_PHASE_MOMENTUM: launch_momentum(c->d, c->P, st, nsm, c->launch); break;
+    case GS_PHASE_VVEL: launch_vvel(c->d, c->P, st, nsm, c->launch); break;
     case GS_PHASE_TRANSPORT: {
-        cudaError_t e = launch_transport(c->d, c->P, c->cfg.dt, st, nsm);
+        cudaError_t e = launch_transport(c->d, c->P, c->cfg.dt, st, nsm, c->launch);
         if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, std::string("transport launch: ") + cudaGetErrorString(e));
         break;
     }
-    case GS_PHASE_LEVELS: launch_levels(c->d, c->P, c->vg, arg, st, nsm); break;
-    case GS_PHASE_NODAL_VEL: launch_nodal_vel(c->d, c->P, st, nsm); break;
+    case GS_PHASE_LEVELS: launch_levels(c->d, c->P, c->vg, arg, st, nsm, c->launch); break;
+    case GS_PHASE_NODAL_VEL: launch_nodal_vel(c->d, c->P, st, nsm, c->launch); break;
     default: return c->fail(GS_ERR_ARG, "unknown phase");
     }
     cudaError_t e = cudaGetLastError();
@@ -748,6 +749,64 @@ gs_status gs_get_stats(gs_ctx* c, int member, gs_stats* out) {
     out->btrack_stops = (int64_t)cnt[1];
     out->error_flags = flags;
     return s == GS_OK ? GS_OK : s;
+}
+
+static_assert((int)GS_K_BTRACK == (int)LK_BTRACK && (int)GS_K_SIDE_PREP == (int)LK_SIDE_PREP &&
+                  (int)GS_K_GHAT == (int)LK_GHAT && (int)GS_K_ASSEMBLE == (int)LK_ASSEMBLE &&
+                  (int)GS_K_MOMENTUM == (int)LK_MOMENTUM && (int)GS_K_VVEL == (int)LK_VVEL &&
+                  (int)GS_K_NODAL_VEL == (int)LK_NODAL_VEL && (int)GS_K_NODAL_TRACER == (int)LK_NODAL_TRACER &&
+                  (int)GS_K_LEVELS == (int)LK_LEVELS && (int)GS_K_JCG_TILES == (int)LK_COUNT,
+              "launch ids of the C ABI");
+
+static int max_threads_of(int kernel, int ntr) {
+    switch (kernel) {
+    case LK_BTRACK: return btrack_max_threads();
+    case LK_SIDE_PREP: case LK_GHAT: case LK_ASSEMBLE: return elev_max_threads(kernel);
+    case LK_MOMENTUM: case LK_VVEL: return mom_max_threads(kernel);
+    case LK_NODAL_VEL: case LK_LEVELS: return levels_max_threads(kernel);
+    case LK_NODAL_TRACER: return transport_max_threads(ntr);
+    default: return 0;
+    }
+}
+
+gs_status gs_set_launch(gs_ctx* c, int kernel, int a, int b) {
+    if (!c || !c->finalized || kernel < 0 || kernel > GS_K_JCG_TILES) return GS_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (kernel == GS_K_JCG_TILES) {
+        // a = tiles of a large member, b = smallest tile (rows, a multiple of 32); the cap of the
+        // cooperative grid stays at its default
+        if (a < 1 || a > 65536 || b < 32 || b > (1 << 24) || b % 32 != 0) return GS_ERR_ARG;
+        JcgTiling tl = c->launch.jcg;
+        tl.tiles = a; tl.min_rows = b;
+        cudaError_t e = cudaStreamSynchronize(c->st);
+        if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+        std::vector<int> row0, rows;
+        for (auto& m : c->mem) { row0.push_back(m.np0); rows.push_back(m.np); }
+        JcgWork* w = nullptr;
+        e = jcg_work_alloc(w, row0, rows, true, c->own_st, tl);
+        if (e != cudaSuccess) {
+            jcg_work_free(w);
+            return c->fail(e == cudaErrorMemoryAllocation ? GS_ERR_OOM : GS_ERR_CUDA, cudaGetErrorString(e));
+        }
+        jcg_work_free(c->jw);
+        c->jw = w;
+        c->launch.jcg = tl;
+    } else {
+        const int mx = max_threads_of(kernel, c->cfg.ntr);
+        if (a < 32 || a % 32 != 0 || a > mx || b < 1 || b > 64) return GS_ERR_ARG;
+        c->launch.k[kernel] = LaunchShape{a, b};
+    }
+    // the captured step holds the old shapes
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    c->graph_vortex = -1;
+    return GS_OK;
+}
+
+gs_status gs_get_launch(gs_ctx* c, int kernel, int* a, int* b) {
+    if (!c || !c->finalized || kernel < 0 || kernel > GS_K_JCG_TILES || !a || !b) return GS_ERR_ARG;
+    if (kernel == GS_K_JCG_TILES) { *a = c->launch.jcg.tiles; *b = c->launch.jcg.min_rows; }
+    else { *a = c->launch.k[kernel].block; *b = c->launch.k[kernel].per_sm; }
+    return GS_OK;
 }
 
 gs_status gs_tracer_mass(gs_ctx* c, int member, double* out) {

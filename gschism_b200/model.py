@@ -169,6 +169,20 @@ class Model:
         L.check(self.lib.gs_get_stats(self.h, member, ctypes.byref(s)), self.h, "gs_get_stats")
         return {f: getattr(s, f) for f, _ in L.GsStats._fields_}
 
+    def set_launch(self, kernel: str, a: int, b: int) -> None:
+        """Launch shape of one kernel (gs_set_launch): threads per block and grid cap in blocks
+        per SM, or for JCG_TILES the tiles of a large member and the smallest tile in rows."""
+        L.check(self.lib.gs_set_launch(self.h, L.LAUNCH[kernel], int(a), int(b)), self.h, f"gs_set_launch {kernel}")
+
+    def get_launch(self, kernel: str):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        L.check(self.lib.gs_get_launch(self.h, L.LAUNCH[kernel], ctypes.byref(a), ctypes.byref(b)), self.h,
+                f"gs_get_launch {kernel}")
+        return a.value, b.value
+
+    def launch_table(self) -> dict:
+        return {k: self.get_launch(k) for k in L.LAUNCH}
+
     def tracer_mass(self, member: int = 0) -> np.ndarray:
         """FP64 tracer mass of a member (sum of prism volume x concentration per tracer,
         compensated, deterministic): gs_tracer_mass."""

@@ -175,7 +175,8 @@ typedef struct {
 gs_status gs_set_vortex(gs_ctx* ctx, int member, const gs_vortex* vortex);
 
 /* Device memory a context holding members of these sizes allocates (bytes, an upper bound used
-   for admission by HBM footprint).  np/ne/ns/nnz are the sums over the members. */
+   for admission by HBM footprint).  np/ne/ns/nnz are the sums over the members.  A TVD context
+   (itr_met = 3) allocates ne * nvrt * ntr * 8 bytes more. */
 size_t gs_footprint_bytes(int nvrt, int ntr, int nmem, int64_t np, int64_t ne, int64_t ns, int64_t nnz);
 
 typedef struct {
@@ -188,6 +189,20 @@ typedef struct {
     int32_t error_flags;       /* device error bits (bounded waits, non-convergence) */
 } gs_stats;
 gs_status gs_get_stats(gs_ctx* ctx, int member, gs_stats* out);
+/* Launch shapes of the step's kernels, for the autotuner (no counterpart in the reference, whose
+   launch shapes are fixed in its kernel wrappers).  For the stream kernels a = threads per block
+   (a multiple of 32, at most what the compiled kernel allows) and b = the grid cap in blocks per
+   SM (1..64); the kernels stride over their entities, so results do not depend on the shape.
+   GS_K_JCG_TILES: a = tiles a large member is cut into, b = the smallest tile in rows (a
+   multiple of 32); this changes the order of the solver's partial sums.  A change takes effect
+   at the next launch (the captured step is recaptured). */
+enum {
+    GS_K_BTRACK = 0, GS_K_SIDE_PREP = 1, GS_K_GHAT = 2, GS_K_ASSEMBLE = 3, GS_K_MOMENTUM = 4,
+    GS_K_VVEL = 5, GS_K_NODAL_VEL = 6, GS_K_NODAL_TRACER = 7, GS_K_LEVELS = 8, GS_K_JCG_TILES = 9
+};
+gs_status gs_set_launch(gs_ctx* ctx, int kernel, int a, int b);
+gs_status gs_get_launch(gs_ctx* ctx, int kernel, int* a, int* b);
+
 /* Tracer mass of a member: for each of the ntr tracers, the sum over the member's wet prisms of
    volume x concentration (out[ntr]), in FP64 with compensated (Neumaier two-sum) accumulation in a
    fixed order, so the value does not depend on the GPU or the launch.  The reference has no mass
