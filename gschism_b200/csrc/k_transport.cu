@@ -71,6 +71,25 @@ __device__ __forceinline__ double tvd_face(int lim, double su, double aq, double
     return psi;
 }
 
+// Minimum of non-negative doubles (compared as their bit patterns) into slot[m] for each lane's
+// member m (m < 0: none): a warp whose lanes share one member reduces with shuffles and issues
+// one atomic, instead of one per element on the same word.  All 32 lanes must call it.
+__device__ __forceinline__ void warp_min_to_member(unsigned long long* slot, int m, double v) {
+    const unsigned full = 0xffffffffu;
+    unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    const int m0 = __shfl_sync(full, m, 0);
+    if (__all_sync(full, m == m0 || m < 0)) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(full, b, o);
+            b = w < b ? w : b;
+        }
+        if ((threadIdx.x & 31) == 0 && m0 >= 0) atomicMin(slot + m0, b);
+    } else if (m >= 0) {
+        atomicMin(slot + m, b);
+    }
+}
+
 // The three sides of element e as the horizontal update needs them (loaded once per element).
 struct ElemSides {
     int s[3], kbs[3], nb[3];
@@ -175,6 +194,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
     const size_t trs = (size_t)nvrt * NE;
     const int G = gridDim.x * blockDim.x;
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;   // blockDim is a multiple of 32: warps start at gid - lane
     const unsigned long long seed = (unsigned long long)__double_as_longlong(1e34);
     for (int m = gid; m < nmem; m += G) {
         T.rem[m] = T.dt; T.rem[nmem + m] = T.dt;
@@ -215,79 +235,87 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
                 }
             }
             if (!grid_sync(d.bar, d.err)) return;
-            // TVD pass 2: admissible sub-step per element
-            for (int e = gid; e < NE; e += G) {
-                const int m = d.elem_member[e];
-                if (!(((volatile double*)T.rem)[par * nmem + m] > 0.0) || d.edry[e]) continue;
-                const ElemSides q = elem_sides(d, e);
+            // TVD pass 2: admissible sub-step per element (warp-uniform loop: the warp reduces
+            // its minimum before the member's atomic)
+            for (int eb = gid - lane; eb < NE; eb += G) {
+                const int e = eb + lane;
+                int mm = -1;
                 double md = kHuge;
-                for (int k = d.kbe[e] + 1; k < nvrt; k++) {
-                    const size_t ix = (size_t)k * NE + e;
-                    const double vol = evol(d, e, k - 1);
-                    double own[NTR], so[NTR], den[NTR];
+                if (e < NE) mm = d.elem_member[e];
+                if (e < NE && ((volatile double*)T.rem)[par * nmem + mm] > 0.0 && !d.edry[e]) {
+                    const ElemSides q = elem_sides(d, e);
+                    for (int k = d.kbe[e] + 1; k < nvrt; k++) {
+                        const size_t ix = (size_t)k * NE + e;
+                        const double vol = evol(d, e, k - 1);
+                        double own[NTR], so[NTR], den[NTR];
 #pragma unroll
-                    for (int t = 0; t < NTR; t++) { own[t] = src[t * trs + ix]; so[t] = 0.0; den[t] = 0.0; }
+                        for (int t = 0; t < NTR; t++) { own[t] = src[t * trs + ix]; so[t] = 0.0; den[t] = 0.0; }
 #pragma unroll
-                    for (int j = 0; j < 3; j++) {
-                        if (k <= q.kbs[j] || !q.nbwet[j]) continue;
-                        const double fq = d.Qh[(size_t)k * NS + q.s[j]];
-                        if (q.sg[j] * fq > 0.0) {
-                            const size_t nx = (size_t)k * NE + q.nb[j];
+                        for (int j = 0; j < 3; j++) {
+                            if (k <= q.kbs[j] || !q.nbwet[j]) continue;
+                            const double fq = d.Qh[(size_t)k * NS + q.s[j]];
+                            if (q.sg[j] * fq > 0.0) {
+                                const size_t nx = (size_t)k * NE + q.nb[j];
 #pragma unroll
-                            for (int t = 0; t < NTR; t++) {
-                                double psir;
-                                tvd_face(lim, d.tvds[t * trs + ix], fabs(fq), own[t], src[t * trs + nx], psir);
-                                so[t] += psir;
+                                for (int t = 0; t < NTR; t++) {
+                                    double psir;
+                                    tvd_face(lim, d.tvds[t * trs + ix], fabs(fq), own[t], src[t * trs + nx], psir);
+                                    so[t] += psir;
+                                }
                             }
                         }
-                    }
 #pragma unroll
-                    for (int j = 0; j < 3; j++) {
-                        if (k <= q.kbs[j] || !q.nbwet[j]) continue;
-                        const double fq = d.Qh[(size_t)k * NS + q.s[j]];
-                        if (q.sg[j] * fq < 0.0) {
-                            const size_t nx = (size_t)k * NE + q.nb[j];
+                        for (int j = 0; j < 3; j++) {
+                            if (k <= q.kbs[j] || !q.nbwet[j]) continue;
+                            const double fq = d.Qh[(size_t)k * NS + q.s[j]];
+                            if (q.sg[j] * fq < 0.0) {
+                                const size_t nx = (size_t)k * NE + q.nb[j];
 #pragma unroll
-                            for (int t = 0; t < NTR; t++) {
-                                double psir;
-                                const double psi = tvd_face(lim, d.tvds[t * trs + nx], fabs(fq), src[t * trs + nx], own[t], psir);
-                                den[t] += fabs(fq) * (1.0 - 0.5 * psi + so[t]);
+                                for (int t = 0; t < NTR; t++) {
+                                    double psir;
+                                    const double psi = tvd_face(lim, d.tvds[t * trs + nx], fabs(fq), src[t * trs + nx], own[t], psir);
+                                    den[t] += fabs(fq) * (1.0 - 0.5 * psi + so[t]);
+                                }
                             }
                         }
-                    }
 #pragma unroll
-                    for (int t = 0; t < NTR; t++) {
-                        const double pd = (den[t] == 0.0) ? kHuge : vol / den[t] * (1.0 - 1.0e-6);
-                        md = fmin(md, pd);
+                        for (int t = 0; t < NTR; t++) {
+                            const double pd = (den[t] == 0.0) ? kHuge : vol / den[t] * (1.0 - 1.0e-6);
+                            md = fmin(md, pd);
+                        }
                     }
+                    d.maxDt[e] = md;
                 }
-                d.maxDt[e] = md;
-                atomicMin(&T.mindt[par * nmem + m], (unsigned long long)__double_as_longlong(md));
+                warp_min_to_member(T.mindt + par * nmem, mm, md);
             }
         } else
         // horizontalAdvectionPrepare (meshdata.cu:6493-6559): inflow and max sub-step per element
-        for (int e = gid; e < NE; e += G) {
-            const int m = d.elem_member[e];
-            if (!(((volatile double*)T.rem)[par * nmem + m] > 0.0) || d.edry[e]) continue;
-            const int kb = d.kbe[e];
-            const ElemSides q = elem_sides(d, e);
+        // (warp-uniform loop: the warp reduces its minimum before the member's atomic)
+        for (int eb = gid - lane; eb < NE; eb += G) {
+            const int e = eb + lane;
+            int mm = -1;
             double md = kHuge;
-            for (int k = kb + 1; k < nvrt; k++) {
-                double in = 0.0;
+            if (e < NE) mm = d.elem_member[e];
+            if (e < NE && ((volatile double*)T.rem)[par * nmem + mm] > 0.0 && !d.edry[e]) {
+                const int kb = d.kbe[e];
+                const ElemSides q = elem_sides(d, e);
+                for (int k = kb + 1; k < nvrt; k++) {
+                    double in = 0.0;
 #pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    if (k <= q.kbs[j]) continue;
-                    if (!q.nbwet[j]) continue;
-                    const double fq = d.Qh[(size_t)k * NS + q.s[j]];
-                    const bool influx = (q.sg[j] * fq) < 0.0;
-                    if (q.bt[j] == 1 || !influx) continue;
-                    in += fabs(fq);
+                    for (int j = 0; j < 3; j++) {
+                        if (k <= q.kbs[j]) continue;
+                        if (!q.nbwet[j]) continue;
+                        const double fq = d.Qh[(size_t)k * NS + q.s[j]];
+                        const bool influx = (q.sg[j] * fq) < 0.0;
+                        if (q.bt[j] == 1 || !influx) continue;
+                        in += fabs(fq);
+                    }
+                    const double pd = (in == 0.0) ? kHuge : evol(d, e, k - 1) / in * (1.0 - 1.0e-6);
+                    md = fmin(md, pd);
                 }
-                const double pd = (in == 0.0) ? kHuge : evol(d, e, k - 1) / in * (1.0 - 1.0e-6);
-                md = fmin(md, pd);
+                d.maxDt[e] = md;
             }
-            d.maxDt[e] = md;
-            atomicMin(&T.mindt[par * nmem + m], (unsigned long long)__double_as_longlong(md));
+            warp_min_to_member(T.mindt + par * nmem, mm, md);
         }
         if (!grid_sync(d.bar, d.err)) return;
         // horizontalAdvectionUpdate (meshdata.cu:6561-6609) with dtb = min(remaining, min maxDt)
