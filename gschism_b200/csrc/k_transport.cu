@@ -188,7 +188,7 @@ __device__ void vertical_upwind(const Dev& d, const Phys& P, int e, double dt, c
         for (int t = 0; t < NTR; t++) dst[t * trs + (size_t)k * NE + e] = up[t];
 }
 
-template <int NTR>
+template <int NTR, bool TVD>
 __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
     const int NE = d.NE, NS = d.NS, nvrt = P.nvrt, nmem = d.nmem;
     const size_t trs = (size_t)nvrt * NE;
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
         const int par = sub & 1, nxt = par ^ 1;
         const double* src = par ? d.prev : d.etr;     // the sub-step's snapshot
         double* dst = par ? d.etr : d.prev;
-        if (P.tvd) {
+        if (TVD) {
             const int lim = P.tvd_limiter;
             // TVD pass 1: inflow sums of the snapshot (interior inflow faces, side order)
             for (int e = gid; e < NE; e += G) {
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
                     if (k <= q.kbs[j]) continue;
                     const double fq = d.Qh[(size_t)k * NS + q.s[j]];
                     const double sQ = q.sg[j] * fq;
-                    if (P.tvd) {
+                    if (TVD) {
                         const int lim = P.tvd_limiter;
                         const double coef = dbv * fabs(fq);
                         const size_t nx = (size_t)k * NE + q.nb[j];
@@ -517,8 +517,11 @@ __global__ void k_nodal_tracer(Dev d, Phys P) {
 
 template <int NTR>
 static cudaError_t launch_ntr(const Dev& d, const Phys& P, TrArgs& T, cudaStream_t st, int nsm, const LaunchShape& nt) {
+    // the TVD passes live in their own instantiation, so the upwind one keeps its smaller
+    // register budget and its occupancy
+    const void* fn = P.tvd ? (const void*)k_transport<NTR, true> : (const void*)k_transport<NTR, false>;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_transport<NTR>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0);
     if (per_sm < 1) per_sm = 1;
     if (per_sm > 4) per_sm = 4;
     int grid = std::min(nsm * per_sm, (d.NE + 255) / 256);
@@ -526,7 +529,7 @@ static cudaError_t launch_ntr(const Dev& d, const Phys& P, TrArgs& T, cudaStream
     Dev dd = d;
     Phys pp = P;
     void* args[] = {&dd, &pp, &T};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_transport<NTR>, dim3(grid), dim3(256), args, 0, st);
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256), args, 0, st);
     if (e != cudaSuccess) return e;
     k_nodal_tracer<NTR><<<grid_of(d.NP, nt, nsm), nt.block, 0, st>>>(d, P);
     return cudaGetLastError();
