@@ -475,43 +475,43 @@ cudaError_t launch_tracer_mass(const Dev& d, const Phys& P, int e0, int e1, doub
 
 template <int NTR>
 __global__ void k_nodal_tracer(Dev d, Phys P) {
-    // nodalTracerUpdate, meshdata.cu:6739-6774 (node-centred gather, no atomics)
-    const int NP = d.NP, NE = d.NE, nvrt = P.nvrt, ivrt = nvrt - 1;
+    // nodalTracerUpdate, meshdata.cu:6739-6774 (node-centred gather, no atomics).  One thread per
+    // (node, level), the level in blockIdx.y; each (node, level) sums its elements in the same
+    // order as a node-by-node loop.
+    const int NP = d.NP, NE = d.NE, nvrt = P.nvrt, ivrt = nvrt - 1, k = blockIdx.y;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NP; i += gridDim.x * blockDim.x) {
         if (d.ndry[i]) continue;
         const int q0 = d.nne_s[i], q1 = d.nne_s[i + 1];
-        for (int k = 0; k < nvrt; k++) {
-            double sum[NTR];
+        double sum[NTR];
 #pragma unroll
-            for (int t = 0; t < NTR; t++) sum[t] = 0.0;
-            double sumA = 0.0;
-            for (int q = q0; q < q1; q++) {
-                const int e = d.nne[q];
-                if (d.edry[e]) continue;
-                const int kb = d.kbe[e];
-                const int kin = k > kb ? k : kb;
-                int kLo = kin, kHi = kin + 1;
-                double zrat = 0.0;
-                if (kin == ivrt) { kLo = ivrt; kHi = ivrt; }
-                else if (kin == kb) { kLo = kb + 1; kHi = kb + 1; }
-                else {
-                    const double zp = d.ez[(size_t)(kin + 1) * NE + e], zc = d.ez[(size_t)kin * NE + e],
-                                 zm = d.ez[(size_t)(kin - 1) * NE + e];
-                    zrat = (zp - zc) / (zp - zm);
-                }
-                const double A = d.area[e];
-#pragma unroll
-                for (int t = 0; t < NTR; t++) {
-                    const double* tr = d.etr + (size_t)t * nvrt * NE;
-                    sum[t] += A * ((1.0 - zrat) * tr[(size_t)kHi * NE + e] + zrat * tr[(size_t)kLo * NE + e]);
-                }
-                sumA += A;
+        for (int t = 0; t < NTR; t++) sum[t] = 0.0;
+        double sumA = 0.0;
+        for (int q = q0; q < q1; q++) {
+            const int e = d.nne[q];
+            if (d.edry[e]) continue;
+            const int kb = d.kbe[e];
+            const int kin = k > kb ? k : kb;
+            int kLo = kin, kHi = kin + 1;
+            double zrat = 0.0;
+            if (kin == ivrt) { kLo = ivrt; kHi = ivrt; }
+            else if (kin == kb) { kLo = kb + 1; kHi = kb + 1; }
+            else {
+                const double zp = d.ez[(size_t)(kin + 1) * NE + e], zc = d.ez[(size_t)kin * NE + e],
+                             zm = d.ez[(size_t)(kin - 1) * NE + e];
+                zrat = (zp - zc) / (zp - zm);
             }
-            if (sumA == 0.0) continue;
-            const double inv = 1.0 / sumA;
+            const double A = d.area[e];
 #pragma unroll
-            for (int t = 0; t < NTR; t++) d.tr[((size_t)t * nvrt + k) * NP + i] = inv * sum[t];
+            for (int t = 0; t < NTR; t++) {
+                const double* tr = d.etr + (size_t)t * nvrt * NE;
+                sum[t] += A * ((1.0 - zrat) * tr[(size_t)kHi * NE + e] + zrat * tr[(size_t)kLo * NE + e]);
+            }
+            sumA += A;
         }
+        if (sumA == 0.0) continue;
+        const double inv = 1.0 / sumA;
+#pragma unroll
+        for (int t = 0; t < NTR; t++) d.tr[((size_t)t * nvrt + k) * NP + i] = inv * sum[t];
     }
 }
 
@@ -531,7 +531,7 @@ static cudaError_t launch_ntr(const Dev& d, const Phys& P, TrArgs& T, cudaStream
     void* args[] = {&dd, &pp, &T};
     cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256), args, 0, st);
     if (e != cudaSuccess) return e;
-    k_nodal_tracer<NTR><<<grid_of(d.NP, nt, nsm), nt.block, 0, st>>>(d, P);
+    k_nodal_tracer<NTR><<<dim3(grid_of(d.NP, nt, nsm), P.nvrt), nt.block, 0, st>>>(d, P);
     return cudaGetLastError();
 }
 
