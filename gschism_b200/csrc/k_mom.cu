@@ -51,7 +51,7 @@ __device__ __forceinline__ double2 slip(double2 u, int8_t bt, double nx, double 
     return t * vtan - nn * vnorm;
 }
 
-__global__ void __launch_bounds__(128) k_momentum(Dev d, Phys P) {
+__global__ void __launch_bounds__(128, 8) k_momentum(Dev d, Phys P) {
     const int NS = d.NS, nvrt = P.nvrt;
     const double dt = P.dt, th = P.thetai;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < NS; s += gridDim.x * blockDim.x) {
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(128) k_momentum(Dev d, Phys P) {
     }
 }
 
-__global__ void __launch_bounds__(128) k_vvel(Dev d, Phys P) {
+__global__ void __launch_bounds__(128, 6) k_vvel(Dev d, Phys P) {
     // computeVerticalVelocity, meshdata.cu:5978-6103 (imm = 0, triangles, ics = 1)
     const int NE = d.NE, NS = d.NS, NP = d.NP, nvrt = P.nvrt;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < NE; e += gridDim.x * blockDim.x) {
