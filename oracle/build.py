@@ -6,6 +6,10 @@
   straight from the reference tree into oracle/_ref/ as the Python module ``test`` it defines
   (pybind11, a METIS stand-in header from oracle/metis_stub).  It runs only where the reference
   tree exists; the built module is a checker for connectivity, never part of the product.
+* ``build_refemu()`` compiles the reference's step kernels for the host (oracle/refemu/build.py)
+  for the 10 km channel case, the library the step fixtures in tests/golden/ come from.
+
+The reference tree is read from $GS_REFERENCE_ROOT (default /root/reference).
 """
 from __future__ import annotations
 
@@ -18,7 +22,7 @@ import sysconfig
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-REFERENCE_ROOT = "/root/reference"
+REFERENCE_ROOT = os.environ.get("GS_REFERENCE_ROOT", "/root/reference")
 LIB = os.path.join(BUILD, "liboracle.so")
 
 
@@ -67,6 +71,17 @@ def build_ref(force: bool = False) -> str | None:
     subprocess.run(cmd, check=True)
     os.replace(tmp, out)
     return out
+
+
+def build_refemu() -> str | None:
+    """The reference's step kernels compiled for the host for the channel case, or None
+    without a reference tree (the fixtures made from it are committed)."""
+    from .refemu import build as rb
+    if not rb.available() or build_ref() is None:
+        return None
+    from gschism_b200 import cases
+    c = cases.channel()
+    return rb.build_for(c, mnond=len(c.open_bnd[0]), mnlnd=len(c.land_bnd[0]))
 
 
 def load_ref():
