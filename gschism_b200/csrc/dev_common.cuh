@@ -64,15 +64,16 @@ __device__ __forceinline__ double2 clampvel(double2 v, double rmaxvel) {
 // to 2^31, so the word's top bit flips exactly when the last block arrives and the low bits are
 // back at zero for the next round.  A waiting block polls until the top bit differs from the one
 // its own add returned: one atomic per block and no reset store.  The wait is bounded: after
-// about 2 s of polling the block records ERR_BARRIER_TIMEOUT and returns false, and every caller
-// then leaves the kernel (the host clears the word before the next launch).
+// `polls` polls (kWaitPolls, about 2 s, unless the context sets another bound) the block records
+// ERR_BARRIER_TIMEOUT and returns false, and every caller then leaves the kernel (the host clears
+// the word and the flag after reporting the timeout).
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 
-__device__ __forceinline__ bool grid_sync(unsigned* bar, int32_t* err) {
+__device__ __forceinline__ bool grid_sync(unsigned* bar, int32_t* err, long long polls) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
@@ -83,7 +84,7 @@ __device__ __forceinline__ bool grid_sync(unsigned* bar, int32_t* err) {
         long long spins = 0;
         while (((ld_acquire_u32(bar) ^ old) & 0x80000000u) == 0u) {
             if (++spins > 4096) __nanosleep(128);
-            if (spins > (1ll << 24)) { atomicOr(err, ERR_BARRIER_TIMEOUT); break; }
+            if (spins > polls) { atomicOr(err, ERR_BARRIER_TIMEOUT); break; }
             if ((spins & 255) == 0 && (*((volatile int32_t*)err) & ERR_BARRIER_TIMEOUT)) break;
         }
         __threadfence();

@@ -20,6 +20,8 @@ void hilbert_order(int n, const double* x, const double* y, std::vector<int32_t>
 
 constexpr int kMaxTracers = 8;
 constexpr int kMaxLevels = 64;
+// default bound of a device wait, in polls: about 2 s of polling
+constexpr long long kWaitPolls = 1ll << 24;
 constexpr int kMaxBfr = 8;
 constexpr int kMaxDeg = 24;        // max node degree supported by the per-row assembly
 constexpr int kVortexParams = 9;  // x0, y0, heading, speed, vmax, rmax, B, rho_air, enabled
@@ -146,7 +148,8 @@ struct Dev {
     // global control
     double* clk;                   // [3] step, time = step * dt, ramp (set on the device each step)
     unsigned* bar;                  // grid barrier word (zero between launches)
-    int32_t *err;
+    int32_t *err;                  // ERR_* flags: set on the device, cleared by the host after reporting
+    long long wait_polls;          // bound of every device wait, in polls (~128 ns each after 4096)
     unsigned long long *counters;  // [4]: walk cap hits, btrack stops, ...
 };
 

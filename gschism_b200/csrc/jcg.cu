@@ -56,7 +56,10 @@ struct JcgView {
     const int32_t* mnblk;          // [nmem] blocks of the refinement grid that hold tiles of the member
     unsigned* ndone;
     unsigned* bar;
-    int32_t* err;
+    int32_t* err;                  // ERR_BARRIER_TIMEOUT (shared with the context's other launches)
+    int32_t* status;               // ERR_JCG_NOT_CONVERGED of this solve (zeroed at every launch)
+    long long wait_polls;          // bound of every wait
+    int stall_member;              // recovery tests: one more arrival expected for this member (-1: none)
     double rtol;
     int maxiter, check_every;
     double inner_rtol;
@@ -198,7 +201,13 @@ __device__ void phase_atol(const JcgView& J, double* sh) {
     }
 }
 
-#define GSYNC() do { if (!grid_sync(J.bar, J.err)) return; } while (0)
+#define GSYNC() do { if (!grid_sync(J.bar, J.err, J.wait_polls)) return; } while (0)
+
+// Arrivals that complete member m's count: its blocks, plus one that never comes when the
+// recovery test stalls the member (its waits then run out and the solve reports a timeout).
+__device__ __forceinline__ unsigned arrivals(const JcgView& J, int m) {
+    return (unsigned)J.mnblk[m] + (m == J.stall_member ? 1u : 0u);
+}
 
 // ------------------------------------------------------------------------------- FP64 ----
 //
@@ -227,7 +236,7 @@ __device__ __forceinline__ int wait64(const JcgView& J, int m, int g, int slot, 
         int cur, st = 1;
         while ((cur = ld_acquire_s32(&J.mgen[m])) < g) {
             if (++spins > 4096) __nanosleep(128);
-            if (spins > (1ll << 24)) { atomicOr(J.err, ERR_BARRIER_TIMEOUT); st = -1; break; }
+            if (spins > J.wait_polls) { atomicOr(J.err, ERR_BARRIER_TIMEOUT); st = -1; break; }
             if ((spins & 255) == 0 && (*((volatile int32_t*)J.err) & ERR_BARRIER_TIMEOUT)) { st = -1; break; }
         }
         __threadfence();
@@ -251,7 +260,7 @@ __device__ __forceinline__ bool arrive64(const JcgView& J, int m, int* shv) {
     if (threadIdx.x == 0) {
         __threadfence();
         const unsigned old = atomicAdd(&J.mcnt[m], 1u);
-        const bool last = ((old + 1u) % (unsigned)J.mnblk[m]) == 0u;
+        const bool last = ((old + 1u) % arrivals(J, m)) == 0u;
         if (last) __threadfence();
         *shv = last ? 1 : 0;
     }
@@ -277,7 +286,7 @@ __device__ void publish_beta(const JcgView& J, int m, int nit, double* sh) {
     if (nit == J.maxiter) {
         // still active after the last iteration: the reference returns maxiter
         J.mdone[m] = J.maxiter;
-        atomicOr(J.err, ERR_JCG_NOT_CONVERGED);
+        atomicOr(J.status, ERR_JCG_NOT_CONVERGED);
         __threadfence();
         atomicAdd(J.ndone, 1u);
         publish64(J, m, kRetired64, 1, 0.0);
@@ -473,7 +482,7 @@ __device__ __forceinline__ void member_wait(const JcgView& J, int m, int it, dou
         bool ok = true;
         while ((g = ld_acquire_i32(&J.mgen[m])) < it) {
             if (++spins > 4096) __nanosleep(128);
-            if (spins > (1ll << 24)) { atomicOr(J.err, ERR_BARRIER_TIMEOUT); ok = false; break; }
+            if (spins > J.wait_polls) { atomicOr(J.err, ERR_BARRIER_TIMEOUT); ok = false; break; }
             if ((spins & 255) == 0 && (*((volatile int32_t*)J.err) & ERR_BARRIER_TIMEOUT)) { ok = false; break; }
         }
         __threadfence();
@@ -497,7 +506,7 @@ __device__ __forceinline__ void member_arrive(const JcgView& J, int m, int it, i
     if (threadIdx.x == 0) {
         __threadfence();
         const unsigned old = atomicAdd(&J.mcnt[m], 1u);
-        const bool last = ((old + 1u) % (unsigned)J.mnblk[m]) == 0u;
+        const bool last = ((old + 1u) % arrivals(J, m)) == 0u;
         if (last) __threadfence();
         *shv = last ? 1 : 0;
     }
@@ -721,7 +730,7 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
         const int m = J.tile_mem[t];
         if (t == J.mem_t0[m] && tid == 0 && ld_done(J, m) < 0) {
             J.mdone[m] = J.minner[m];
-            atomicOr(J.err, ERR_JCG_NOT_CONVERGED);
+            atomicOr(J.status, ERR_JCG_NOT_CONVERGED);
         }
     }
 }
@@ -734,8 +743,10 @@ struct JcgWork {
     int32_t *tile_r0 = nullptr, *tile_r1 = nullptr, *tile_mem = nullptr, *mem_t0 = nullptr, *mem_t1 = nullptr;
     int32_t *blk64 = nullptr, *blkir = nullptr;
     double *tile_part = nullptr, *mem_atol2 = nullptr, *mem_ab = nullptr;
-    // per-member control words in one array: mdone, mouter, minner, mret, mgen, mcnt ([nmem] each), ndone
+    // per-member control words in one array: mdone, mouter, minner, mret, mgen, mcnt ([nmem] each),
+    // ndone, status (ERR_JCG_NOT_CONVERGED of the last solve)
     int32_t* mctl = nullptr;
+    int32_t* status = nullptr;
     int32_t *mdone = nullptr, *mouter = nullptr, *minner = nullptr, *mret = nullptr, *mgen = nullptr;
     unsigned* mcnt = nullptr;
     int32_t *mnblk = nullptr, *mnblk64 = nullptr;   // blocks holding each member's tiles (IR, FP64 grids)
@@ -821,6 +832,7 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     w->mdone = w->mctl; w->mouter = w->mctl + nmem; w->minner = w->mctl + 2 * nmem; w->mret = w->mctl + 3 * nmem;
     w->mgen = w->mctl + 4 * nmem; w->mcnt = (unsigned*)(w->mctl + 5 * nmem);
     w->ndone = (unsigned*)(w->mctl + 6 * nmem);
+    w->status = w->mctl + 6 * nmem + 1;
     {
         // blocks of each grid holding tiles of each member
         auto count = [&](const std::vector<int32_t>& bt, int grid, int32_t* dst) {
@@ -873,11 +885,13 @@ cudaError_t jcg_launch(const JcgArgs& a, JcgWork* w, cudaStream_t st, int nsm) {
     J.mdone = w->mdone; J.mouter = w->mouter; J.minner = w->minner; J.mret = w->mret; J.ndone = w->ndone;
     J.mem_ab = w->mem_ab; J.mpub = w->mem_ab + 4 * (size_t)w->nmem;
     J.mgen = w->mgen; J.mcnt = w->mcnt; J.mnblk = ir ? w->mnblk : w->mnblk64;
-    J.bar = a.bar; J.err = a.err;
+    J.bar = a.bar; J.err = a.err; J.status = w->status;
+    J.wait_polls = a.wait_polls > 0 ? a.wait_polls : kWaitPolls;
+    J.stall_member = (a.stall_member >= 0 && a.stall_member < w->nmem) ? a.stall_member : -1;
     J.rtol = a.rtol; J.maxiter = a.maxiter; J.check_every = a.check_every > 0 ? a.check_every : 1;
     J.inner_rtol = a.inner_rtol; J.inner_maxiter = a.inner_maxiter;
     cudaMemsetAsync(w->mdone, 0xFF, 4 * (size_t)w->nmem, st);
-    cudaMemsetAsync(w->mouter, 0, 4 * (5 * (size_t)w->nmem + 1), st);   // mouter .. mcnt, ndone
+    cudaMemsetAsync(w->mouter, 0, 4 * (5 * (size_t)w->nmem + 2), st);   // mouter .. mcnt, ndone, status
     void* args[] = {&J};
     if ((a.sell != nullptr) != w->sell) return cudaErrorInvalidValue;
     const void* fn = ir ? (w->sell ? (const void*)k_jcg_ir<true> : (const void*)k_jcg_ir<false>)
@@ -895,6 +909,11 @@ cudaError_t jcg_read_iters(JcgWork* w, std::vector<int>& iters, std::vector<int>
 }
 
 int32_t* jcg_iters_device(JcgWork* w) { return w->mdone; }
+
+cudaError_t jcg_read_status(JcgWork* w, int32_t* flags, cudaStream_t st) {
+    cudaMemcpyAsync(flags, w->status, 4, cudaMemcpyDeviceToHost, st);
+    return cudaStreamSynchronize(st);
+}
 
 // ------------------------------------------------------------- solve without allocating ----
 //
@@ -920,7 +939,7 @@ constexpr size_t kNoAllocBytes = kNaOffCtl + kNaCtlBytes;                // abou
 static __device__ __align__(256) unsigned char gs_noalloc_scratch[kNoAllocBytes];
 
 // control words at kNaOffCtl: [0] mem_t0, [1] mem_t1, [2] mdone, [3] mouter, [4] ndone,
-// [5] grid barrier word, [6] unused, [7] err, [8] mgen, [9] mcnt, [10] mnblk (= grid: every
+// [5] grid barrier word, [6] solve status, [7] err, [8] mgen, [9] mcnt, [10] mnblk (= grid: every
 // block holds tiles of the one member); published scalars at kNaOffAtol + 64
 
 __global__ void k_noalloc_setup(unsigned char* base, int n, const int32_t* indptr, const int32_t* indices,
@@ -1001,7 +1020,8 @@ extern "C" gs_status gs_jcg_solve_csr_noalloc(int n, const int32_t* indptr, cons
     J.blk_t0 = (const int32_t*)(base + kNaOffBlk);
     J.mem_t0 = ctl + 0; J.mem_t1 = ctl + 1; J.mdone = ctl + 2; J.mouter = ctl + 3;
     J.ndone = (unsigned*)(ctl + 4); J.bar = (unsigned*)(ctl + 5);
-    J.err = ctl + 7;
+    J.err = ctl + 7; J.status = ctl + 6;
+    J.wait_polls = kWaitPolls; J.stall_member = -1;
     J.mgen = ctl + 8; J.mcnt = (unsigned*)(ctl + 9); J.mnblk = ctl + 10;
     J.mpub = (double*)(base + kNaOffAtol + 64);
     J.rtol = rtol; J.maxiter = maxiter; J.check_every = check_every > 0 ? check_every : 1;
@@ -1016,6 +1036,3 @@ extern "C" gs_status gs_jcg_solve_csr_noalloc(int n, const int32_t* indptr, cons
     if (h[7] & ERR_BARRIER_TIMEOUT) return GS_ERR_TIMEOUT;
     return GS_OK;
 }
-
-namespace gs {
-}  // namespace gs

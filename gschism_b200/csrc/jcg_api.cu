@@ -138,6 +138,7 @@ gs_status gs_jcg_solve_csr(gs_jcg* s, double rtol, int maxiter, int check_every,
     a.bar = s->bar; a.err = s->err;
     a.rtol = rtol; a.maxiter = maxiter; a.check_every = check_every < 1 ? 1 : check_every;
     a.inner_rtol = 0.1; a.inner_maxiter = 400;
+    a.wait_polls = kWaitPolls; a.stall_member = -1;
     cudaError_t e = jcg_launch(a, s->w, s->st, s->nsm);
     if (e != cudaSuccess) { s->msg = cudaGetErrorString(e); return GS_ERR_CUDA; }
     k_roll<<<g, 256, 0, s->st>>>(n, s->x, s->x0, s->x1, s->x2);
@@ -149,7 +150,9 @@ gs_status gs_jcg_solve_csr(gs_jcg* s, double rtol, int maxiter, int check_every,
     cudaStreamSynchronize(s->st);
     if (iters) *iters = it[0];
     if (flags & ERR_BARRIER_TIMEOUT) {
-        cudaMemsetAsync(s->bar, 0, sizeof(unsigned), s->st);     // the barrier word is left mid-round
+        // the barrier word is left mid-round; both words are cleared so the next solve starts clean
+        cudaMemsetAsync(s->bar, 0, sizeof(unsigned), s->st);
+        cudaMemsetAsync(s->err, 0, sizeof(int32_t), s->st);
         cudaStreamSynchronize(s->st);
         s->msg = "device barrier timed out";
         return GS_ERR_TIMEOUT;

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
         T.nsub[m] = 0;
     }
     if (gid == 0) *T.active = (unsigned)nmem;
-    if (!grid_sync(d.bar, d.err)) return;
+    if (!grid_sync(d.bar, d.err, d.wait_polls)) return;
     for (int sub = 0; sub < T.maxsub; sub++) {
         if (*((volatile unsigned*)T.active) == 0u) break;
         const int par = sub & 1, nxt = par ^ 1;
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
                     for (int t = 0; t < NTR; t++) d.tvds[t * trs + ix] = su[t];
                 }
             }
-            if (!grid_sync(d.bar, d.err)) return;
+            if (!grid_sync(d.bar, d.err, d.wait_polls)) return;
             // TVD pass 2: admissible sub-step per element (warp-uniform loop: the warp reduces
             // its minimum before the member's atomic)
             for (int eb = gid - lane; eb < NE; eb += G) {
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
             }
             warp_min_to_member(T.mindt + par * nmem, mm, md);
         }
-        if (!grid_sync(d.bar, d.err)) return;
+        if (!grid_sync(d.bar, d.err, d.wait_polls)) return;
         // horizontalAdvectionUpdate (meshdata.cu:6561-6609) with dtb = min(remaining, min maxDt)
         for (int e = gid; e < NE; e += G) {
             const int m = d.elem_member[e];
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
                 for (int k = 0; k <= kb; k++) dst[t * trs + (size_t)k * NE + e] = v;
             }
         }
-        if (!grid_sync(d.bar, d.err)) return;
+        if (!grid_sync(d.bar, d.err, d.wait_polls)) return;
     }
     // verticalAdvectionUpdate for every wet element, once its member has finished sub-cycling:
     // after n sub-steps the horizontal result is in prev when n is odd, in etr when it is even

@@ -26,6 +26,8 @@ struct JcgArgs {
     int maxiter, check_every;
     double inner_rtol;
     int inner_maxiter;
+    long long wait_polls;                // bound of every wait of the solve (0: kWaitPolls)
+    int stall_member;                    // recovery tests: this member's arrivals never complete (-1: off)
 };
 struct JcgWork;
 cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std::vector<int>& rows, bool sell,
@@ -33,6 +35,8 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
 void jcg_work_free(JcgWork* w);
 cudaError_t jcg_launch(const JcgArgs& a, JcgWork* w, cudaStream_t st, int nsm);
 cudaError_t jcg_read_iters(JcgWork* w, std::vector<int>& iters, std::vector<int>& outer, cudaStream_t st);
+// ERR_JCG_NOT_CONVERGED of the last solve (cleared at every launch); 0 or the flag
+cudaError_t jcg_read_status(JcgWork* w, int32_t* flags, cudaStream_t st);
 int32_t* jcg_iters_device(JcgWork* w);
 
 // k_elev.cu

@@ -92,6 +92,7 @@ struct gs_ctx {
     LaunchTable launch;              // launch shapes (defaults or the autotuner's)
     double* mass_part = nullptr;     // tracer mass budget: per-block partials and result
     double* mass_out = nullptr;
+    int stall_member = -1;           // recovery tests: the member whose solve waits run out
     gs_status fail(gs_status s, const std::string& m) { err = m; return s; }
 };
 
@@ -552,6 +553,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     UP(vort, c->h_vort);
     AL(mem_rem, 2 * (size_t)d.nmem); AL(mem_dtb, d.nmem); AL(mem_mindt, 2 * (size_t)d.nmem + 1); AL(mem_nsub, d.nmem);
     AL(clk, 3); AL(bar, 1); AL(err, 1); AL(counters, 4);
+    d.wait_polls = kWaitPolls;
     if (e == cudaSuccess) e = dalloc(c, c->mass_part, (size_t)kMassBlocks * kMaxTracers * 2);
     if (e == cudaSuccess) e = dalloc(c, c->mass_out, (size_t)kMaxTracers);
 #undef UP
@@ -611,6 +613,7 @@ static gs_status run_phase(gs_ctx* c, int phase, int arg) {
         a.bar = d.bar; a.err = d.err;
         a.rtol = c->cfg.rtol; a.maxiter = c->cfg.maxiter; a.check_every = c->cfg.check_every;
         a.inner_rtol = c->cfg.ir_inner_rtol; a.inner_maxiter = c->cfg.ir_inner_maxiter;
+        a.wait_polls = c->d.wait_polls; a.stall_member = c->stall_member;
         cudaError_t e = jcg_launch(a, c->jw, st, nsm);
         if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, std::string("jcg launch: ") + cudaGetErrorString(e));
         break;
@@ -637,11 +640,15 @@ static gs_status check_err(gs_ctx* c) {
     cudaError_t e = cudaMemcpyAsync(&flags, c->d.err, 4, cudaMemcpyDeviceToHost, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
     if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
-    if (flags & ERR_BARRIER_TIMEOUT) {
-        cudaMemsetAsync(c->d.bar, 0, sizeof(unsigned), c->st);   // the barrier word is left mid-round
-        return c->fail(GS_ERR_TIMEOUT, "a bounded device barrier timed out");
+    if (flags & (ERR_BARRIER_TIMEOUT | ERR_DEGREE)) {
+        // reported once: the barrier word (left mid-round by a timeout) and the flags are cleared,
+        // so the context's next launches start clean
+        cudaMemsetAsync(c->d.bar, 0, sizeof(unsigned), c->st);
+        cudaMemsetAsync(c->d.err, 0, sizeof(int32_t), c->st);
+        cudaStreamSynchronize(c->st);
+        if (flags & ERR_BARRIER_TIMEOUT) return c->fail(GS_ERR_TIMEOUT, "a bounded device wait timed out");
+        return c->fail(GS_ERR_BAD_MESH, "node degree above the supported maximum");
     }
-    if (flags & ERR_DEGREE) return c->fail(GS_ERR_BAD_MESH, "node degree above the supported maximum");
     return GS_OK;
 }
 
@@ -736,11 +743,14 @@ gs_status gs_get_stats(gs_ctx* c, int member, gs_stats* out) {
     cudaError_t e = jcg_read_iters(c->jw, iters, outer, c->st);
     if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
     unsigned long long cnt[4] = {0, 0, 0, 0};
-    int32_t nsub = 0, flags = 0;
+    int32_t nsub = 0, flags = 0, jflags = 0;
     cudaMemcpyAsync(cnt, c->d.counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->st);
     cudaMemcpyAsync(&nsub, c->d.mem_nsub + member, 4, cudaMemcpyDeviceToHost, c->st);
     cudaMemcpyAsync(&flags, c->d.err, 4, cudaMemcpyDeviceToHost, c->st);
     cudaStreamSynchronize(c->st);
+    jcg_read_status(c->jw, &jflags, c->st);
+    flags |= jflags;   // non-convergence of the last solve (ERR_BARRIER_TIMEOUT was reported above)
+    if (s == GS_ERR_TIMEOUT) flags |= ERR_BARRIER_TIMEOUT;
     std::memset(out, 0, sizeof(*out));
     out->jcg_iters = iters[member];
     out->jcg_outer = outer[member];
@@ -797,6 +807,23 @@ gs_status gs_set_launch(gs_ctx* c, int kernel, int a, int b) {
         c->launch.k[kernel] = LaunchShape{a, b};
     }
     // the captured step holds the old shapes
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    c->graph_vortex = -1;
+    return GS_OK;
+}
+
+gs_status gs_set_wait_limit(gs_ctx* c, long long polls) {
+    if (!c || !c->finalized || polls < 0) return GS_ERR_ARG;
+    c->d.wait_polls = polls > 0 ? polls : kWaitPolls;
+    // the captured step holds the old bound in its kernel parameters
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    c->graph_vortex = -1;
+    return GS_OK;
+}
+
+gs_status gs_test_stall_solve(gs_ctx* c, int member) {
+    if (!c || !c->finalized || member < -1 || member >= (int)c->mem.size()) return GS_ERR_ARG;
+    c->stall_member = member;
     if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
     c->graph_vortex = -1;
     return GS_OK;

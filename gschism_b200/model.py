@@ -157,6 +157,15 @@ class Model:
     def phase(self, name: str, arg: int = 0) -> None:
         L.check(self.lib.gs_phase(self.h, L.PHASE[name], int(arg)), self.h, f"gs_phase {name}")
 
+    def set_wait_limit(self, polls: int) -> None:
+        """Bound of the device waits in polls (gs_set_wait_limit; 0 = the default, about 2 s)."""
+        L.check(self.lib.gs_set_wait_limit(self.h, int(polls)), self.h, "gs_set_wait_limit")
+
+    def test_stall_solve(self, member: int) -> None:
+        """Recovery tests only (gs_test_stall_solve): the member's next solves wait for an arrival
+        that never comes, so their bounded waits run out; -1 switches it off."""
+        L.check(self.lib.gs_test_stall_solve(self.h, int(member)), self.h, "gs_test_stall_solve")
+
     def set_stream(self, stream_ptr: int | None) -> None:
         """Issue the member work on a caller cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""
         L.check(self.lib.gs_set_stream(self.h, ctypes.c_void_p(stream_ptr or None)), self.h, "gs_set_stream")

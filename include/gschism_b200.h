@@ -208,6 +208,22 @@ gs_status gs_get_launch(gs_ctx* ctx, int kernel, int* a, int* b);
    fixed order, so the value does not depend on the GPU or the launch.  The reference has no mass
    budget; this is the FP64 budget the mass-conservation checks read. */
 gs_status gs_tracer_mass(gs_ctx* ctx, int member, double* out);
+
+/* Bound of every device wait of the context's persistent kernels (the grid barrier of the
+ * transport and the solver's member-level waits), in polls: after 4,096 plain polls each poll
+ * sleeps about 128 ns, so the default (0 selects it: 2^24 polls) is about 2 s.  A wait that runs
+ * out sets a flag; every block then leaves its kernel, later launches of the step return at
+ * once, and the next gs_sync / gs_get_stats / gs_state_get returns GS_ERR_TIMEOUT and clears the
+ * flag and the barrier word, so the context is usable again (its state is that of an unfinished
+ * step: put a saved state back before stepping on).  No counterpart in the reference, whose
+ * native solver loop bounds its host-side wait by `timeout_seconds` (pcg_loop.cpp:182-291). */
+gs_status gs_set_wait_limit(gs_ctx* ctx, long long polls);
+
+/* For tests of the recovery path only: the next solves of `member` wait for one block arrival
+ * that never comes, so their bounded waits run out (see gs_set_wait_limit) and the step reports
+ * GS_ERR_TIMEOUT; -1 switches it off.  No device fault or endless wait is involved.  No
+ * counterpart in the reference. */
+gs_status gs_test_stall_solve(gs_ctx* ctx, int member);
 /* sizes of a member: np, ne, ns, nnz (CSR of the elevation matrix) */
 gs_status gs_member_sizes(gs_ctx* ctx, int member, int* np, int* ne, int* ns, int* nnz);
 

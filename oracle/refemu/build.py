@@ -6,7 +6,9 @@ For one case this script
      namelist, into oracle/_ref/refemu/<tag>/constants.h;
   2. compiles oracle/refemu/ref_step.cpp, which includes src/kernels/meshdata.cu unchanged from
      the reference tree, with g++ (asserts on, FMA contraction off) into
-     oracle/_ref/refemu/<tag>/libref_step.so.
+     oracle/_ref/refemu/<tag>/libref_step.so; with fma=True the same source is compiled with
+     multiply-adds contracted into FMA instructions (-mfma -ffp-contract=fast), as nvcc/NVRTC
+     contract the reference's kernels by default on a GPU.
 The include order makes the generated constants.h win over the one that sits beside
 meshdata.cu (-I<tag> -I<kernels> -I-: quote includes search these directories only, in this
 order) and oracle/refemu/cuda_runtime.h stand in for the CUDA runtime header.
@@ -78,7 +80,7 @@ def _varcodes() -> str:
     return re.search(r"enum class VarCode \{([^}]*)\}", txt).group(1)
 
 
-def build_for(case, mnond: int, mnlnd: int) -> str:
+def build_for(case, mnond: int, mnlnd: int, fma: bool = False) -> str:
     """constants.h + libref_step.so for this case; returns the library path."""
     tmpl = open(os.path.join(kernels_dir(), "constants_template.h")).read()
     vals = constants_for(case, mnond, mnlnd)
@@ -90,7 +92,8 @@ def build_for(case, mnond: int, mnlnd: int) -> str:
         raise RuntimeError(f"constants template placeholders left unfilled: {left}")
     src = os.path.join(HERE, "ref_step.cpp")
     shim = os.path.join(HERE, "cuda_runtime.h")
-    key = hashlib.sha1((tmpl + open(src).read() + open(shim).read()).encode()).hexdigest()[:12]
+    fp = ["-mfma", "-ffp-contract=fast"] if fma else ["-ffp-contract=off"]
+    key = hashlib.sha1((tmpl + open(src).read() + open(shim).read() + " ".join(fp)).encode()).hexdigest()[:12]
     d = os.path.join(OUT, key)
     lib = os.path.join(d, "libref_step.so")
     if os.path.exists(lib):
@@ -99,7 +102,7 @@ def build_for(case, mnond: int, mnlnd: int) -> str:
     with open(os.path.join(d, "constants.h"), "w") as f:
         f.write(tmpl)
     tmp = lib + f".tmp{os.getpid()}"
-    cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-w",
+    cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared"] + fp + ["-w",
            "-include", shim, "-I", d, "-I", kernels_dir(), "-I-", "-I", HERE, src, "-o", tmp]
     subprocess.run(cmd, check=True)
     os.replace(tmp, lib)

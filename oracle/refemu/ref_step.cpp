@@ -81,9 +81,9 @@ RefModel* g_model = nullptr;
  * two runs that differ only in it bound how far the reference departs from itself. */
 int g_atomic_order = 0;
 
-/* Summation order of the solver's dot products: 0 = sequential, 1 = blocked (sequential sums
- * of 256 entries, then the block sums added pairwise), the shape of a GPU library reduction.
- * The reference's dot products run in cuBLAS/CuPy, whose order is not specified. */
+/* Summation order of the solver's dot products: 0 = sequential, 1 = warp-shaped (sequential
+ * sums of 32 entries, then the partial sums added pairwise), the shape of a GPU library
+ * reduction.  The reference's dot products run in cuBLAS/CuPy, whose order is not specified. */
 int g_dot_order = 0;
 
 double dot_sum(const double* a, const double* b, int n) {
@@ -93,9 +93,9 @@ double dot_sum(const double* a, const double* b, int n) {
         return s;
     }
     std::vector<double> part;
-    for (int i0 = 0; i0 < n; i0 += 256) {
+    for (int i0 = 0; i0 < n; i0 += 32) {
         double s = 0.0;
-        const int i1 = i0 + 256 < n ? i0 + 256 : n;
+        const int i1 = i0 + 32 < n ? i0 + 32 : n;
         for (int i = i0; i < i1; ++i) s += a[i] * b[i];
         part.push_back(s);
     }

@@ -74,11 +74,14 @@ def _quiet(fn):
 class RefStep:
     """One case stepped by the reference's kernels on the CPU."""
 
-    def __init__(self, case, rtol=None, maxiter=None, check_every=None, quiet=True, atomic_order=0, dot_order=0):
+    def __init__(self, case, rtol=None, maxiter=None, check_every=None, quiet=True, atomic_order=0, dot_order=0,
+                 fma=False):
         """atomic_order 1 runs the kernels whose sums are atomic updates (nodal velocities,
         open-boundary velocities, boundary areas) in reversed thread order; dot_order 1 sums the
-        solver's dot products in 256-entry blocks added pairwise.  Both are orders a GPU run of
-        the reference may take, so runs that differ in them show its own reproducibility."""
+        solver's dot products in 32-entry blocks added pairwise; fma compiles the kernels with
+        contracted multiply-adds.  Each is a choice a GPU run of the reference makes (thread
+        order, library reduction order, nvcc's default contraction), so runs that differ in them
+        show the reference's own reproducibility."""
         self.case = case
         self.quiet = quiet
         ref = _ob.load_ref() if os.path.exists(_ob.ref_module_path()) else None
@@ -97,7 +100,7 @@ class RefStep:
         nope, mnond = np.asarray(iond).shape
         nland, mnlnd = np.asarray(ilnd).shape
         self.grid = dict(elside=np.asarray(elside), isdel=np.asarray(isdel), isidenode=np.asarray(isidenode))
-        lib_path = _b.build_for(case, mnond, mnlnd)
+        lib_path = _b.build_for(case, mnond, mnlnd, fma=fma)
         self.L = L = ctypes.CDLL(lib_path)
         L.rd_create.argtypes = [ctypes.POINTER(RefInput)]
         L.rd_kernel.argtypes = [ctypes.c_char_p, ctypes.c_double, ctypes.c_int, ctypes.c_int]

@@ -8,9 +8,10 @@ reference tree (oracle/refemu/build.py) and driven in the order of src/python/sc
   steps (fields of meshes above 300 nodes on a fixed seeded subset of entities, all levels), with the JCG
   iteration count and transport sub-step count of every step;
 * the reference's reproducibility envelope: for every snapshot field, the largest relative
-  difference between this run and two runs that differ only in summation orders a GPU run of the
-  reference may take (its atomic nodal-velocity sums in reversed thread order; its solver dot
-  products in blocked pairwise order);
+  difference between this run and three runs that differ only in choices a GPU run of the
+  reference makes (its atomic nodal-velocity sums in reversed thread order; its solver dot
+  products in 32-entry blocks added pairwise; its kernels compiled with contracted
+  multiply-adds, as nvcc/NVRTC do by default);
 * for the cases with `phase_step`, the complete state before that step and every phase's output
   within it, for per-phase checks from an identical state.
 
@@ -42,8 +43,8 @@ PHASE_OUT = {
     "BTRACK": ("SIDE_BTU",),
     "PREPARE": ("ELBC", "SIDE_U", "SIDE_HHAT", "SIDE_CHI", "ELEM_GHAT"),
     "ASSEMBLE": ("CSR_DATA", "QEL"),
-    "SOLVE": ("JCG_X",),
-    "UPDATE_ELEV": ("ETA2", "NODE_KB"),
+    "SOLVE": (),
+    "UPDATE_ELEV": ("ETA2", "NODE_KB", "JCG_X"),
     "MOMENTUM": ("SIDE_U2",),
     "VVEL": ("ELEM_W", "ELEM_QV"),
     "TRANSPORT": ("SIDE_QH", "ELEM_TR", "NODE_TR"),
@@ -95,15 +96,15 @@ def _cut(name, a, sub):
     return a[:, idx]
 
 
-def _run_variant(name, atomic_order, dot_order, out):
+def _run_variant(name, atomic_order, dot_order, fma, out):
     """Child process: one reference run (the mesh is a process-wide global there)."""
     from oracle.refemu.refstep import RefStep
     c, nsteps, snaps, phase_step = step_cases()[name]
     sub = subset_indices(c)
-    r = RefStep(c, atomic_order=atomic_order, dot_order=dot_order)
+    r = RefStep(c, atomic_order=atomic_order, dot_order=dot_order, fma=bool(fma))
     res = {"iters": [], "substeps": []}
     for it in range(1, nsteps + 1):
-        if phase_step is not None and it == phase_step and atomic_order == 0 and dot_order == 0:
+        if phase_step is not None and it == phase_step and atomic_order == 0 and dot_order == 0 and not fma:
             for f in STATE_FIELDS:
                 res[f"state_{f}"] = r.get(f)
             time = r.begin_step(it)
@@ -141,12 +142,12 @@ def _rel(a, b):
 def make(name):
     with tempfile.TemporaryDirectory() as d:
         outs = {}
-        for tag, ao, do in (("base", 0, 0), ("atomic", 1, 0), ("dots", 0, 1)):
+        for tag, ao, do, fm in (("base", 0, 0, 0), ("atomic", 1, 0, 0), ("dots", 0, 1, 0), ("fma", 0, 0, 1)):
             outs[tag] = os.path.join(d, f"{tag}.npz")
-            subprocess.run([sys.executable, os.path.abspath(__file__), "--variant", name, str(ao), str(do),
+            subprocess.run([sys.executable, os.path.abspath(__file__), "--variant", name, str(ao), str(do), str(fm),
                             outs[tag]], check=True, stdout=subprocess.DEVNULL)
         base = dict(np.load(outs["base"]))
-        var = [dict(np.load(outs[t])) for t in ("atomic", "dots")]
+        var = [dict(np.load(outs[t])) for t in ("atomic", "dots", "fma")]
     c, nsteps, snaps, phase_step = step_cases()[name]
     if phase_step is not None:
         base["phase_step"] = np.int32(phase_step)
@@ -166,7 +167,7 @@ def make(name):
 
 def main(argv):
     if len(argv) >= 2 and argv[1] == "--variant":
-        _run_variant(argv[2], int(argv[3]), int(argv[4]), argv[5])
+        _run_variant(argv[2], int(argv[3]), int(argv[4]), int(argv[5]), argv[6])
         return
     names = argv[1:] or list(step_cases())
     for n in names:
