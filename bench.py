@@ -16,6 +16,12 @@ The plain FP64 single-instance form is measured on the same GPU and reported und
 ensemble = the batched form: 64 members on meshes of uneven size (20k-500k nodes, 20 levels,
            1 tracer, per-member tide and wind), all members in one launch per phase, FP32+IR and
            FP64, against the plain FP64 single-instance form run member by member.
+error_vs_oracle = the FP64 and FP32+IR forms after 3 steps of the benchmarked mesh against the
+           CPU oracle (oracle/, pinned to the reference's own kernels by tests/test_ref_pinned.py)
+           after the same 3 steps: elevation max |difference| in m, tracers and velocities relative.
+cpu_baseline = the oracle on the benchmarked mesh itself (all host threads), 2 timed steps.
+--impl reference = the same oracle on the benchmarked mesh, 1 warm-up + up to 6 timed steps (a
+           bounded sample of the run), plus a single-thread figure on a 200 x 200 sample.
 Multi-GPU (torchrun): every rank steps its own replica of the mesh (no data exchange exists in
 the step); value = all ranks' node-level-steps / the max over ranks of the device time.
 """
@@ -263,7 +269,9 @@ def run_ours(a):
     if srv is not None:
         line["serving"] = srv
     if not a.no_cpu:
-        line["cpu_baseline"] = cpu_sample(a)
+        cb, ofields, case_full = cpu_sample(a)
+        line["cpu_baseline"] = cb
+        line["error_vs_oracle"] = error_vs_oracle(case_full, ofields, 3, local)
     print(json.dumps(line))
 
 
@@ -294,18 +302,66 @@ def run_ensemble(a, stream, local):
     out = {"workload": f"64 members, {nodes} nodes in total (20k-500k each, log-uniform), {nvrt} levels, "
                        f"1 tracer, per-member tide 0.3-2 m and wind stress 0-0.3 N/m2, dt=120 s",
            "nodes": nodes, "levels": nvrt, "steps": steps, "warmup": warm}
+    phases = ["BEGIN", "BTRACK", "PREPARE", "ASSEMBLE", "SOLVE", "UPDATE_ELEV", "MOMENTUM", "VVEL", "TRANSPORT",
+              "LEVELS", "NODAL_VEL"]
+    peak, peak_kind = _peaks()
+
+    def breakdown(m, it0, nstep=2):
+        """Device time of every phase over `nstep` steps issued phase by phase (CUDA events on the
+        launching stream), in ms per step, and the per-member solver counters of the last step."""
+        acc = {p: 0.0 for p in phases}
+        for k in range(nstep):
+            evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(phases) + 1)]
+            evs[0].record(stream)
+            for i, p in enumerate(phases):
+                m.phase(p, it0 + k)
+                evs[i + 1].record(stream)
+            torch.cuda.synchronize()
+            for i, p in enumerate(phases):
+                acc[p] += evs[i].elapsed_time(evs[i + 1]) / nstep
+        st = [m.stats(i) for i in range(len(ens))]
+        return acc, st
+
     eta = {}
+    small = sorted(range(len(ens)), key=lambda i: ens[i].n_nodes)[:2]
     for prec in ("fp32_ir", "fp64"):
         m = Model(ens, precision=prec, device=local)
         ms = timed(m)
         its = [m.stats(i)["jcg_iters"] for i in range(len(ens))]
         eta[prec] = [m.get(i, "ETA2").copy() for i in range(len(ens))]
+        ph, st = breakdown(m, warm + steps + 1)
+        # roofline of the batched solve: algorithmic bytes of every member's iterations / phase time
+        byts = 0.0
+        for i, sz in enumerate(m.sizes):
+            if prec == "fp32_ir":
+                byts += st[i]["jcg_iters"] * _jcg_bytes_per_iter(sz["np"], sz["nnz"], "fp32") + \
+                    st[i]["jcg_outer"] * (sz["nnz"] * 12 + 4 * sz["np"] + 3 * 8 * sz["np"])
+            else:
+                byts += st[i]["jcg_iters"] * _jcg_bytes_per_iter(sz["np"], sz["nnz"], "fp64")
+        ach = byts / (ph["SOLVE"] / 1e3) / 1e9
         out[f"{prec}_batched"] = {"value": nodes * nvrt / (ms / 1e3), "ms_per_step": ms,
-                                  "jcg_iters_min": min(its), "jcg_iters_max": max(its)}
+                                  "jcg_iters_min": min(its), "jcg_iters_max": max(its),
+                                  "phase_ms": {p: round(v, 3) for p, v in ph.items()},
+                                  "solve_roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                                                     "frac": ach / peak, "peak_kind": peak_kind,
+                                                     "bytes_per_launch": byts,
+                                                     "kernel": "k_jcg_ir" if prec == "fp32_ir" else "k_jcg64"}}
         m.close()
         del m
         torch.cuda.empty_cache()
     out["max_eta_diff_fp32_ir_vs_fp64_m"] = max(float(np.max(np.abs(x - y))) for x, y in zip(eta["fp32_ir"], eta["fp64"]))
+    # the two smallest members (their own tide and wind) against the CPU oracle, same steps
+    from oracle.step_api import OracleModel
+    errs = []
+    for i in small:
+        o = OracleModel(ens[i])
+        o.run(warm + steps)
+        oe = o.get("ETA2")
+        errs.append({"member": i, "nodes": int(ens[i].n_nodes),
+                     "fp32_ir_eta_max_abs_m": float(np.abs(eta["fp32_ir"][i] - oe).max()),
+                     "fp64_eta_max_abs_m": float(np.abs(eta["fp64"][i] - oe).max())})
+        del o
+    out["error_vs_oracle"] = {"steps": warm + steps, "members": errs}
     tot = 0.0
     for c in ens:
         m = Model([c], precision="fp64", device=local)
@@ -337,45 +393,125 @@ def run_serving(local, n=8, rate=2.0, hours=6.0, seed=1):
     return out
 
 
-def cpu_sample(a, steps=6, n=500):
-    """The CPU restatement (oracle) on a bounded sample of the same workload: a n x n basin with
-    the same levels, tracers and physics, all host threads, `steps` steps."""
+def _cpu_info():
+    """Host CPU model and logical core count (recorded beside every CPU number)."""
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return model, os.cpu_count() or 1
+
+
+def _omp_threads(n):
+    """Set the OpenMP thread count of the already loaded oracle library (libgomp)."""
+    import ctypes
+    try:
+        ctypes.CDLL("libgomp.so.1").omp_set_num_threads(int(n))
+        return True
+    except OSError:
+        return False
+
+
+def _fields_of(get):
+    return {f: np.array(get(f), copy=True) for f in ("ETA2", "ELEM_TR", "SIDE_U2")}
+
+
+def _errors(g, o):
+    def rel(x, y):
+        s_ = float(np.abs(y).max())
+        return float(np.abs(x - y).max()) / (s_ if s_ > 0 else 1.0)
+    return {"eta_max_abs_m": float(np.abs(g["ETA2"] - o["ETA2"]).max()),
+            "tracer_rel": rel(g["ELEM_TR"], o["ELEM_TR"]), "velocity_rel": rel(g["SIDE_U2"], o["SIDE_U2"])}
+
+
+def cpu_sample(a, steps=3):
+    """The CPU oracle on the benchmarked mesh itself (all host threads): step 1 untimed, steps
+    2..`steps` timed.  Returns the cpu_baseline entry and the oracle's fields after `steps` steps
+    (the error_vs_oracle comparison)."""
     from gschism_b200 import cases
     from oracle.step_api import OracleModel
-    case = cases.basin(seed=2, n=n, nvrt=30, nz=10, ntr=2, length=500e3 * n / 1000)
+    case = cases.basin(seed=2, n=a.n, nvrt=30, nz=10, ntr=2)
     o = OracleModel(case)
+    o.run(1)
     t0 = time.perf_counter()
-    o.run(steps)
+    o.run(steps - 1, start=2)
     dtm = time.perf_counter() - t0
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": case.n_nodes * case.nvrt * steps / dtm, "unit": METRIC, "cores": cores, "kind": "port",
-            "sample": f"basin {n}x{n} ({case.n_nodes} nodes), 30 levels, 2 tracers, {steps} steps, {dtm:.1f} s"}
+    fields = _fields_of(o.get)
+    cpu, ncores = _cpu_info()
+    cores = int(os.environ.get("OMP_NUM_THREADS", ncores))
+    out = {"value": case.n_nodes * case.nvrt * (steps - 1) / dtm, "unit": METRIC, "cores": cores, "kind": "port",
+           "sample": f"the benchmarked basin {a.n}x{a.n} ({case.n_nodes} nodes, 30 levels, 2 tracers): steps 2-{steps} "
+                     f"timed after one untimed step, {dtm:.1f} s", "cpu_model": cpu}
+    del o
+    return out, fields, case
+
+
+def error_vs_oracle(case, oracle_fields, steps, device):
+    """The FP64 and FP32+IR forms after `steps` steps of `case` against the oracle's fields after
+    the same steps."""
+    from gschism_b200.model import Model
+    out = {"workload": f"the benchmarked mesh ({case.n_nodes} nodes), {steps} steps from the cold start",
+           "oracle": "oracle/ (CPU FP64 restatement, pinned to the reference's own kernels)"}
+    for prec in ("fp64", "fp32_ir"):
+        m = Model([case], precision=prec, device=device)
+        m.step(steps)
+        m.sync()
+        out[prec] = _errors(_fields_of(lambda f: m.get(0, f)), oracle_fields)
+        m.close()
+        del m
+    out["fp32_ir_within_1e-6_m"] = out["fp32_ir"]["eta_max_abs_m"] <= 1e-6
+    return out
 
 
 def run_reference(a):
+    """The reference arm: the CPU oracle (the reference has no CPU path of its own; the oracle is
+    pinned to its kernels) on the benchmarked mesh, all host threads, 1 warm-up step and up to 6
+    timed steps; plus one step single-threaded on a 200 x 200 sample."""
     ws, rank, local = _dist()
     if rank != 0:
         return
     from gschism_b200 import cases
     from oracle.step_api import OracleModel
-    n = 500
-    case = cases.basin(seed=2, n=n, nvrt=30, nz=10, ntr=2, length=500e3 * n / 1000)
+    case = cases.basin(seed=2, n=a.n, nvrt=30, nz=10, ntr=2)
     o = OracleModel(case)
-    for _ in range(min(a.warmup, 1)):
-        o.run(1)
+    warm = max(1, min(a.warmup, 1))
+    o.run(warm)
+    k = max(1, min(a.steps, 6))
     t0 = time.perf_counter()
-    o.run(a.steps)
+    o.run(k, start=warm + 1)
     dtm = time.perf_counter() - t0
-    v = case.n_nodes * case.nvrt * a.steps / dtm
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    sample = (f"CPU restatement of the reference kernels (the reference has no CPU path): basin {n}x{n} "
-              f"({case.n_nodes} nodes), 30 levels, 2 tracers, {a.steps} steps")
+    del o
+    v = case.n_nodes * case.nvrt * k / dtm
+    cpu, ncores = _cpu_info()
+    cores = int(os.environ.get("OMP_NUM_THREADS", ncores))
+    single = None
+    small = cases.basin(seed=2, n=200, nvrt=30, nz=10, ntr=2, length=500e3 * 200 / 1000)
+    if _omp_threads(1):
+        o1 = OracleModel(small)
+        o1.run(1)
+        t1 = time.perf_counter()
+        o1.run(1, start=2)
+        d1 = time.perf_counter() - t1
+        single = {"value": small.n_nodes * small.nvrt / d1, "unit": METRIC, "cores": 1,
+                  "sample": f"basin 200x200 ({small.n_nodes} nodes), 30 levels, 2 tracers, step 2 after one untimed step"}
+        _omp_threads(cores)
+        del o1
+    sample = (f"CPU oracle (the reference has no CPU path; the oracle is pinned to the reference's own kernels): "
+              f"the benchmarked basin {a.n}x{a.n} ({case.n_nodes} nodes), 30 levels, 2 tracers, {k} timed steps "
+              f"after {warm} warm-up step")
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": ws, "steps": a.steps,
-        "warmup": a.warmup, "ms_per_step": dtm / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": ws, "steps": k,
+        "warmup": warm, "ms_per_step": dtm / k * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"basin {a.n}x{a.n} nodes, 30 SZ levels, 2 tracers, dt=120 s (sampled at {n}x{n})"},
-        "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample},
+        "config": {"workload": f"basin {a.n}x{a.n} nodes ({case.n_nodes}), 30 SZ levels, 2 tracers, dt=120 s, "
+                               f"JCG rtol 1e-12", "nodes": case.n_nodes, "levels": case.nvrt,
+                   "parallelism": f"{cores} host threads"},
+        "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample,
+                         "cpu_model": cpu, "single_thread": single},
         "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 

@@ -29,7 +29,8 @@ EXPORTS = ["gs_grid_build", "gs_ctx_create", "gs_member_add", "gs_ctx_prepare", 
            "gs_last_error", "gs_sync", "gs_set_stream", "gs_step", "gs_phase", "gs_state_get", "gs_state_put", "gs_set_tau",
            "gs_get_stats", "gs_tracer_mass", "gs_set_launch", "gs_get_launch", "gs_member_sizes", "gs_jcg_create", "gs_jcg_buffers", "gs_jcg_solve_csr",
            "gs_jcg_check", "gs_jcg_destroy", "gs_jcg_last_error", "gs_jcg_solve_csr_noalloc",
-           "gs_set_vortex", "gs_footprint_bytes", "gs_set_wait_limit", "gs_test_stall_solve"]
+           "gs_set_vortex", "gs_footprint_bytes", "gs_set_wait_limit", "gs_test_stall_solve", "gs_state_get_async",
+           "gs_output_mark", "gs_output_wait", "gs_host_alloc", "gs_host_free"]
 
 
 class GsConfig(ctypes.Structure):
@@ -113,9 +114,15 @@ def load(build_if_missing: bool = False):
     L.gs_set_vortex.argtypes = [c_void_p, I, ctypes.POINTER(GsVortex)]
     L.gs_set_wait_limit.argtypes = [c_void_p, ctypes.c_longlong]
     L.gs_test_stall_solve.argtypes = [c_void_p, I]
+    L.gs_state_get_async.argtypes = [c_void_p, I, I, c_void_p, c_size_t]
+    L.gs_output_mark.argtypes = [c_void_p, ctypes.POINTER(ctypes.c_uint64)]
+    L.gs_output_wait.argtypes = [c_void_p, ctypes.c_uint64]
+    L.gs_host_alloc.argtypes = [c_size_t]
+    L.gs_host_alloc.restype = c_void_p
+    L.gs_host_free.argtypes = [c_void_p]
     L.gs_footprint_bytes.argtypes = [I, I, I, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64]
     for name in EXPORTS:
-        if name not in ("gs_last_error", "gs_jcg_last_error", "gs_footprint_bytes"):
+        if name not in ("gs_last_error", "gs_jcg_last_error", "gs_footprint_bytes", "gs_host_alloc"):
             getattr(L, name).restype = c_int
     L.gs_footprint_bytes.restype = c_size_t
     _lib = L

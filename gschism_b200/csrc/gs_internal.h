@@ -26,7 +26,7 @@ constexpr int kMaxBfr = 8;
 constexpr int kMaxDeg = 24;        // max node degree supported by the per-row assembly
 constexpr int kVortexParams = 9;  // x0, y0, heading, speed, vmax, rmax, B, rho_air, enabled
 constexpr int kMassBlocks = 256;    // fixed grid of the tracer mass budget (deterministic sums)
-constexpr int kIrVectors = 10;     // FP32 vectors of the refinement solve: (u, w, s, -) x 2, p, d
+constexpr int kIrVectors = 9;      // FP32 vectors of the refinement solve: (u, w, s, p) x 2, d
 
 // Device error bits (gs_stats.error_flags)
 enum : int {
@@ -84,6 +84,8 @@ struct Dev {
     int NP, NE, NS, NNZ, NB, nmem;
     // nodes
     double *x, *y, *depth, *drag, *tau, *eta1, *eta2, *qel, *elbc;
+    double *tau_own;               // [NP][2] the members' own surface stress (restored after a storm)
+    int32_t *pn_ref, *ps_ref, *pe_ref;   // internal entity -> reference index within its member
     int32_t *kb;
     uint8_t *ndry, *nwas, *ess;
     int32_t *nbnd;                 // -1 interior, -2 land-only, >= 0 open

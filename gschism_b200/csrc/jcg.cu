@@ -441,14 +441,19 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
 // (u_i, w~_i, s~_{i-1}), so u, w~ and s~ are double-buffered by iteration parity and no barrier
 // separates the vector update from the matrix product.
 
-// FP32 vectors in ir32: (u, w~, s~, unused) packed per row for iteration parities 0 and 1
-// (4 n floats each, so a neighbour's three values arrive in one 16-byte load), then p and d.
-static_assert(kIrVectors == 10, "ir32 layout");
+// FP32 vectors in ir32: (u, w~, s~, p) packed per row for iteration parities 0 and 1 (4 n floats
+// each, so a neighbour's three values arrive in one 16-byte load and a row's own four in one),
+// then d.
+static_assert(kIrVectors == 9, "ir32 layout");
+
+// resident blocks per SM the refinement solve is compiled for (register budget)
+#ifndef GS_JCG_IR_MIN_BLOCKS
+#define GS_JCG_IR_MIN_BLOCKS 4
+#endif
 __device__ __forceinline__ float4* ir_uws(const JcgView& J, int parity) {
     return reinterpret_cast<float4*>(J.ir32) + (size_t)parity * J.n;
 }
-__device__ __forceinline__ float* ir_p(const JcgView& J) { return J.ir32 + (size_t)8 * J.n; }
-__device__ __forceinline__ float* ir_d(const JcgView& J) { return J.ir32 + (size_t)9 * J.n; }
+__device__ __forceinline__ float* ir_d(const JcgView& J) { return J.ir32 + (size_t)8 * J.n; }
 
 // u_{i+1} of a row from its (u_i, w~_i, s~_{i-1}); the same expression for a row and its neighbours
 __device__ __forceinline__ float u_next(float4 q, float al, float bt) { return q.x - al * (q.y + bt * q.z); }
@@ -548,14 +553,13 @@ __device__ __forceinline__ void member_arrive(const JcgView& J, int m, int it, i
 }
 
 template <bool SELL>
-__global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
+__global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgView J) {
     __shared__ double sh[4 * 32];
     __shared__ double pub[3];
     __shared__ int shv;
     const int tid = threadIdx.x;
     const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
     const int nmem = J.nmem;
-    float* const pp = ir_p(J);
     float* const dd = ir_d(J);
     phase_bb(J, sh);
     GSYNC();
@@ -588,9 +592,10 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
                 for (int i = r0 + tid; i < r1; i += kThreads) {
                     const double s = row_dot<SELL, double>(J, J.A, i, [&](int c) { return J.x[c]; });
                     const double ri = J.b[i] - s;
-                    const float sprev = (outer > 0) ? uwl[i].z : 0.0f;
-                    uw0[i] = make_float4((float)(J.invD[i] * ri), 0.0f, sprev, 0.0f);
-                    if (outer == 0) pp[i] = 0.0f;
+                    // s~ and p of the previous sweep's last iteration (zero in the first sweep)
+                    float sprev = 0.0f, pprev = 0.0f;
+                    if (outer > 0) { const float4 l = uwl[i]; sprev = l.z; pprev = l.w; }
+                    uw0[i] = make_float4((float)(J.invD[i] * ri), 0.0f, sprev, pprev);
                     dd[i] = 0.0f;
                     v[0] += ri * ri;
                 }
@@ -698,14 +703,14 @@ __global__ void __launch_bounds__(kThreads) k_jcg_ir(JcgView J) {
                 const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
                 double v[3] = {0.0, 0.0, 0.0};
                 for (int i = r0 + tid; i < r1; i += kThreads) {
+                    // a row's (u, w~, s~, p) travel together: one 16-byte load and store per row
                     const float4 o = uwc[i];
                     const float snew = o.y + bt * o.z;
-                    const float pnew = o.x + bt * pp[i];
+                    const float pnew = o.x + bt * o.w;
                     dd[i] += al * pnew;
-                    pp[i] = pnew;
                     const float unew = u_next(o, al, bt);
                     const float w = row_dot<SELL, float>(J, J.A32, i, [&](int c) { return u_next(uwc[c], al, bt); });
-                    uwn[i] = make_float4(unew, w, snew, 0.0f);
+                    uwn[i] = make_float4(unew, w, snew, pnew);
                     const double dg = J.diag32[i], du = dg * unew;
                     v[0] += du * unew; v[1] += dg * (double)w * unew; v[2] += du * du;
                 }

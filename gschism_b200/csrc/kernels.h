@@ -39,6 +39,12 @@ cudaError_t jcg_read_iters(JcgWork* w, std::vector<int>& iters, std::vector<int>
 cudaError_t jcg_read_status(JcgWork* w, int32_t* flags, cudaStream_t st);
 int32_t* jcg_iters_device(JcgWork* w);
 
+// k_xfer.cu: one member's field between device slices and a reference-ordered block
+void launch_gather(const void* src, void* dst, int kind, int n, int N, int off, int nslices, int nc,
+                   const int32_t* perm, const int32_t* remap, cudaStream_t st, int nsm);
+void launch_scatter(const void* src, void* dst, int kind, int n, int N, int off, int nslices, int nc,
+                    const int32_t* perm, cudaStream_t st, int nsm);
+
 // k_elev.cu
 void launch_clock_set(const Dev& d, const Phys& P, int it, cudaStream_t st);
 void launch_clock_advance(const Dev& d, const Phys& P, cudaStream_t st);

@@ -5,6 +5,8 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -93,6 +95,20 @@ struct gs_ctx {
     double* mass_part = nullptr;     // tracer mass budget: per-block partials and result
     double* mass_out = nullptr;
     int stall_member = -1;           // recovery tests: the member whose solve waits run out
+    // field exchange staging: one device block, two pinned host blocks used in turn (an event
+    // per host block marks when its last copy has finished)
+    void* dstage = nullptr;
+    size_t dstage_bytes = 0;
+    void* hstage[2] = {nullptr, nullptr};
+    size_t hstage_bytes[2] = {0, 0};
+    cudaEvent_t hev[2] = {nullptr, nullptr};
+    int hnext = 0;
+    // output marks (gs_output_mark / gs_output_wait): ticket -> event, and recycled events; a
+    // writer thread may wait on a mark while the stepping thread records the next ones
+    std::mutex marks_mu;
+    uint64_t next_ticket = 1;
+    std::map<uint64_t, cudaEvent_t> marks;
+    std::vector<cudaEvent_t> free_events;
     gs_status fail(gs_status s, const std::string& m) { err = m; return s; }
 };
 
@@ -524,7 +540,16 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     cudaError_t e = cudaSuccess;
 #define UP(field, vec) if (e == cudaSuccess) e = dup(c, d.field, vec)
 #define AL(field, n) if (e == cudaSuccess) e = dalloc(c, d.field, n)
-    UP(x, B.x); UP(y, B.y); UP(depth, B.depth); UP(drag, B.drag); UP(tau, B.tau);
+    UP(x, B.x); UP(y, B.y); UP(depth, B.depth); UP(drag, B.drag); UP(tau, B.tau); UP(tau_own, B.tau);
+    {
+        std::vector<int32_t> pn(NP), ps(NS), pe(NE);
+        for (const MemberHost& m : c->mem) {
+            for (int i = 0; i < m.np; i++) pn[m.np0 + i] = m.pn[i];
+            for (int i = 0; i < m.con.ns; i++) ps[m.ns0 + i] = m.ps[i];
+            for (int i = 0; i < m.ne; i++) pe[m.ne0 + i] = m.pe[i];
+        }
+        UP(pn_ref, pn); UP(ps_ref, ps); UP(pe_ref, pe);
+    }
     AL(eta1, NP); AL(eta2, NP); AL(qel, NP); AL(elbc, NP); AL(kb, NP); AL(ndry, NP); AL(nwas, NP);
     UP(ess, B.ess); UP(nbnd, B.nbnd);
     AL(z, (size_t)nvrt * NP); AL(w2, (size_t)nvrt * NP); AL(u2, (size_t)nvrt * NP);
@@ -856,6 +881,13 @@ gs_status gs_ctx_destroy(gs_ctx* c) {
     if (c->own_st) cudaStreamDestroy(c->own_st);
     jcg_work_free(c->jw);
     for (void* p : c->allocs) cudaFree(p);
+    if (c->dstage) cudaFree(c->dstage);
+    for (int k = 0; k < 2; k++) {
+        if (c->hstage[k]) cudaFreeHost(c->hstage[k]);
+        if (c->hev[k]) cudaEventDestroy(c->hev[k]);
+    }
+    for (auto& kv : c->marks) cudaEventDestroy(kv.second);
+    for (cudaEvent_t ev : c->free_events) cudaEventDestroy(ev);
     delete c;
     return GS_OK;
 }
@@ -938,6 +970,70 @@ void member_csr(gs_ctx* c, MemberHost& m, std::vector<int32_t>& indptr, std::vec
     (void)C;
 }
 
+// One member's field as the exchange kernels see it (k_xfer.cu).
+struct Block {
+    int kind, n, N, off, nslices, nc;
+    const int32_t* perm;
+};
+
+gs_status field_block(gs_ctx* c, const MemberHost& m, const FieldInfo& fi, size_t bytes, Block& k) {
+    const Dev& d = c->d;
+    k.kind = fi.isint == 2 ? 2 : (fi.isint ? 1 : 0);
+    k.N = fi.ent == 'N' ? d.NP : fi.ent == 'S' ? d.NS : d.NE;
+    k.n = fi.ent == 'N' ? m.np : fi.ent == 'S' ? m.con.ns : m.ne;
+    k.off = fi.ent == 'N' ? m.np0 : fi.ent == 'S' ? m.ns0 : m.ne0;
+    k.perm = (fi.ent == 'N' ? d.pn_ref : fi.ent == 'S' ? d.ps_ref : d.pe_ref) + k.off;
+    k.nc = fi.comp == 2 ? 2 : 1;
+    k.nslices = (fi.comp == -1 ? c->cfg.ntr : 1) * (fi.lev ? c->cfg.nvrt : 1);
+    const size_t esz = fi.isint ? 4 : 8;
+    if (bytes != (size_t)k.nslices * k.n * k.nc * esz) return c->fail(GS_ERR_STATE, "size mismatch for field");
+    return GS_OK;
+}
+
+// Staging blocks of at least `bytes`: the device block and the next pinned host block (after its
+// previous copy has finished).  Grows them on demand.
+cudaError_t stage(gs_ctx* c, size_t bytes, int& h) {
+    cudaError_t e = cudaSuccess;
+    if (c->dstage_bytes < bytes) {
+        if (c->dstage) { cudaStreamSynchronize(c->st); cudaFree(c->dstage); }
+        c->dstage = nullptr; c->dstage_bytes = 0;
+        e = cudaMalloc(&c->dstage, bytes);
+        if (e != cudaSuccess) return e;
+        c->dstage_bytes = bytes;
+    }
+    h = c->hnext;
+    c->hnext ^= 1;
+    if (!c->hev[h]) {
+        e = cudaEventCreateWithFlags(&c->hev[h], cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    } else {
+        e = cudaEventSynchronize(c->hev[h]);
+        if (e != cudaSuccess) return e;
+    }
+    if (c->hstage_bytes[h] < bytes) {
+        if (c->hstage[h]) cudaFreeHost(c->hstage[h]);
+        c->hstage[h] = nullptr; c->hstage_bytes[h] = 0;
+        e = cudaHostAlloc(&c->hstage[h], bytes, cudaHostAllocDefault);
+        if (e != cudaSuccess) return e;
+        c->hstage_bytes[h] = bytes;
+    }
+    return cudaSuccess;
+}
+
+// Host block (reference order) -> device field, stream-ordered: the caller's buffer is copied to
+// pinned staging before the call returns, the upload and the scatter run on the context stream.
+cudaError_t put_block(gs_ctx* c, const void* host, size_t bytes, void* dst, const Block& k) {
+    int h = 0;
+    cudaError_t e = stage(c, bytes, h);
+    if (e != cudaSuccess) return e;
+    std::memcpy(c->hstage[h], host, bytes);
+    e = cudaMemcpyAsync(c->dstage, c->hstage[h], bytes, cudaMemcpyHostToDevice, c->st);
+    if (e != cudaSuccess) return e;
+    cudaEventRecord(c->hev[h], c->st);
+    launch_scatter(c->dstage, dst, k.kind, k.n, k.N, k.off, k.nslices, k.nc, k.perm, c->st, c->nsm);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 extern "C" gs_status gs_state_get(gs_ctx* c, int member, int field, void* host, size_t bytes) {
@@ -945,9 +1041,8 @@ extern "C" gs_status gs_state_get(gs_ctx* c, int member, int field, void* host, 
     FieldInfo fi;
     if (!field_info(c, field, fi)) return c->fail(GS_ERR_STATE, "unknown field");
     MemberHost& m = c->mem[member];
-    const int nvrt = c->cfg.nvrt, ntr = c->cfg.ntr;
-    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->fail(GS_ERR_CUDA, "sync");
     if (fi.ent == 'C' || fi.ent == 'R') {
+        if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->fail(GS_ERR_CUDA, "sync");
         std::vector<int32_t> ip, ix, src;
         member_csr(c, m, ip, ix, src);
         if (fi.ent == 'R') {
@@ -966,35 +1061,85 @@ extern "C" gs_status gs_state_get(gs_ctx* c, int member, int field, void* host, 
         }
         return GS_OK;
     }
-    const int N = fi.ent == 'N' ? c->d.NP : fi.ent == 'S' ? c->d.NS : c->d.NE;
-    const int n = fi.ent == 'N' ? m.np : fi.ent == 'S' ? m.con.ns : m.ne;
-    const int off = fi.ent == 'N' ? m.np0 : fi.ent == 'S' ? m.ns0 : m.ne0;
-    const std::vector<int32_t>& perm = fi.ent == 'N' ? m.pn : fi.ent == 'S' ? m.ps : m.pe;   // new -> old
-    const int nl = fi.lev ? nvrt : 1;
-    const int nc = fi.comp == 2 ? 2 : 1;
-    const int nt = fi.comp == -1 ? ntr : 1;
-    const size_t esz = fi.isint ? 4 : 8;
-    const size_t need = (size_t)nt * nl * n * nc * esz;
-    if (bytes != need) return c->fail(GS_ERR_STATE, "size mismatch for field");
-    const size_t dsz = fi.isint == 2 ? 1 : esz;
-    std::vector<char> buf((size_t)n * nc * dsz);
-    for (int t = 0; t < nt; t++)
-        for (int k = 0; k < nl; k++) {
-            const size_t dev_off = (((size_t)t * nl + k) * N + off) * nc * dsz;
-            cudaMemcpyAsync(buf.data(), (char*)fi.ptr + dev_off, buf.size(), cudaMemcpyDeviceToHost, c->st);
-            cudaStreamSynchronize(c->st);
-            for (int i = 0; i < n; i++) {
-                const int o = perm[i];
-                const size_t dst = ((((size_t)t * nl + k) * n + o) * nc) * esz;
-                if (fi.isint == 2) ((int32_t*)((char*)host + dst))[0] = (int32_t)(uint8_t)buf[i];
-                else std::memcpy((char*)host + dst, buf.data() + (size_t)i * nc * dsz, nc * dsz);
-                if (field == GS_F_SIDE_BTELEM) {       // element ids back to reference numbering
-                    int32_t* v = (int32_t*)((char*)host + dst);
-                    if (*v >= 0) *v = m.pe[*v - m.ne0];
-                }
-            }
-        }
+    Block k;
+    gs_status st = field_block(c, m, fi, bytes, k);
+    if (st != GS_OK) return st;
+    int h = 0;
+    cudaError_t e = stage(c, bytes, h);
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    launch_gather(fi.ptr, c->dstage, k.kind, k.n, k.N, k.off, k.nslices, k.nc, k.perm,
+                  field == GS_F_SIDE_BTELEM ? c->d.pe_ref : nullptr, c->st, c->nsm);
+    e = cudaMemcpyAsync(c->hstage[h], c->dstage, bytes, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    std::memcpy(host, c->hstage[h], bytes);
     return GS_OK;
+}
+
+extern "C" gs_status gs_state_get_async(gs_ctx* c, int member, int field, void* host, size_t bytes) {
+    if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size() || !host) return GS_ERR_ARG;
+    FieldInfo fi;
+    if (!field_info(c, field, fi)) return c->fail(GS_ERR_STATE, "unknown field");
+    if (fi.ent == 'C' || fi.ent == 'R') return c->fail(GS_ERR_STATE, "CSR fields have no asynchronous read");
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, host) != cudaSuccess || pa.type != cudaMemoryTypeHost) {
+        cudaGetLastError();
+        return c->fail(GS_ERR_ARG, "gs_state_get_async needs page-locked host memory (gs_host_alloc)");
+    }
+    Block k;
+    gs_status st = field_block(c, c->mem[member], fi, bytes, k);
+    if (st != GS_OK) return st;
+    cudaError_t e = cudaSuccess;
+    if (c->dstage_bytes < bytes) {
+        if (c->dstage) { cudaStreamSynchronize(c->st); cudaFree(c->dstage); }
+        c->dstage = nullptr; c->dstage_bytes = 0;
+        e = cudaMalloc(&c->dstage, bytes);
+        if (e != cudaSuccess) return c->fail(GS_ERR_OOM, cudaGetErrorString(e));
+        c->dstage_bytes = bytes;
+    }
+    launch_gather(fi.ptr, c->dstage, k.kind, k.n, k.N, k.off, k.nslices, k.nc, k.perm,
+                  field == GS_F_SIDE_BTELEM ? c->d.pe_ref : nullptr, c->st, c->nsm);
+    e = cudaMemcpyAsync(host, c->dstage, bytes, cudaMemcpyDeviceToHost, c->st);
+    return e == cudaSuccess ? GS_OK : c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+extern "C" gs_status gs_output_mark(gs_ctx* c, uint64_t* ticket) {
+    if (!c || !c->finalized || !ticket) return GS_ERR_ARG;
+    std::lock_guard<std::mutex> lk(c->marks_mu);
+    cudaEvent_t ev = nullptr;
+    if (!c->free_events.empty()) { ev = c->free_events.back(); c->free_events.pop_back(); }
+    else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return GS_ERR_CUDA;
+    if (cudaEventRecord(ev, c->st) != cudaSuccess) { c->free_events.push_back(ev); return GS_ERR_CUDA; }
+    *ticket = c->next_ticket++;
+    c->marks[*ticket] = ev;
+    return GS_OK;
+}
+
+extern "C" gs_status gs_output_wait(gs_ctx* c, uint64_t ticket) {
+    if (!c || !c->finalized) return GS_ERR_ARG;
+    cudaEvent_t ev = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(c->marks_mu);
+        auto it = c->marks.find(ticket);
+        if (it == c->marks.end()) return GS_ERR_ARG;
+        ev = it->second;
+        c->marks.erase(it);
+    }
+    const cudaError_t e = cudaEventSynchronize(ev);
+    std::lock_guard<std::mutex> lk(c->marks_mu);
+    c->free_events.push_back(ev);
+    return e == cudaSuccess ? GS_OK : GS_ERR_CUDA;
+}
+
+extern "C" void* gs_host_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0 || cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    return p;
+}
+
+extern "C" gs_status gs_host_free(void* p) {
+    if (!p) return GS_ERR_ARG;
+    return cudaFreeHost(p) == cudaSuccess ? GS_OK : GS_ERR_CUDA;
 }
 
 extern "C" gs_status gs_state_put(gs_ctx* c, int member, int field, const void* host, size_t bytes) {
@@ -1002,43 +1147,28 @@ extern "C" gs_status gs_state_put(gs_ctx* c, int member, int field, const void* 
     FieldInfo fi;
     if (!field_info(c, field, fi)) return c->fail(GS_ERR_STATE, "unknown field");
     if (fi.ent == 'C' || fi.ent == 'R') return c->fail(GS_ERR_STATE, "CSR fields are read-only");
-    MemberHost& m = c->mem[member];
-    const int nvrt = c->cfg.nvrt, ntr = c->cfg.ntr;
-    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->fail(GS_ERR_CUDA, "sync");
-    const int N = fi.ent == 'N' ? c->d.NP : fi.ent == 'S' ? c->d.NS : c->d.NE;
-    const int n = fi.ent == 'N' ? m.np : fi.ent == 'S' ? m.con.ns : m.ne;
-    const int off = fi.ent == 'N' ? m.np0 : fi.ent == 'S' ? m.ns0 : m.ne0;
-    const std::vector<int32_t>& perm = fi.ent == 'N' ? m.pn : fi.ent == 'S' ? m.ps : m.pe;
-    const int nl = fi.lev ? nvrt : 1;
-    const int nc = fi.comp == 2 ? 2 : 1;
-    const int nt = fi.comp == -1 ? ntr : 1;
-    const size_t esz = fi.isint ? 4 : 8;
-    if (bytes != (size_t)nt * nl * n * nc * esz) return c->fail(GS_ERR_STATE, "size mismatch for field");
-    const size_t dsz = fi.isint == 2 ? 1 : esz;
-    std::vector<char> buf((size_t)n * nc * dsz);
-    for (int t = 0; t < nt; t++)
-        for (int k = 0; k < nl; k++) {
-            for (int i = 0; i < n; i++) {
-                const int o = perm[i];
-                const size_t src = ((((size_t)t * nl + k) * n + o) * nc) * esz;
-                if (fi.isint == 2) buf[i] = (char)(uint8_t)((const int32_t*)((const char*)host + src))[0];
-                else std::memcpy(buf.data() + (size_t)i * nc * dsz, (const char*)host + src, nc * dsz);
-            }
-            const size_t dev_off = (((size_t)t * nl + k) * N + off) * nc * dsz;
-            cudaMemcpyAsync((char*)fi.ptr + dev_off, buf.data(), buf.size(), cudaMemcpyHostToDevice, c->st);
-            cudaStreamSynchronize(c->st);
-        }
+    Block k;
+    gs_status st = field_block(c, c->mem[member], fi, bytes, k);
+    if (st != GS_OK) return st;
+    cudaError_t e = put_block(c, host, bytes, fi.ptr, k);
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
     return GS_OK;
 }
 
 extern "C" gs_status gs_set_tau(gs_ctx* c, int member, const double* tau_host) {
     if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size() || !tau_host) return GS_ERR_ARG;
-    MemberHost& m = c->mem[member];
-    m.tau.assign(tau_host, tau_host + 2 * (size_t)m.np);        // restored when a storm is switched off
-    std::vector<double> buf(2 * (size_t)m.np);
-    for (int i = 0; i < m.np; i++) { buf[2 * i] = tau_host[2 * m.pn[i]]; buf[2 * i + 1] = tau_host[2 * m.pn[i] + 1]; }
-    cudaError_t e = cudaMemcpyAsync(c->d.tau + 2 * (size_t)m.np0, buf.data(), buf.size() * 8, cudaMemcpyHostToDevice, c->st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    FieldInfo fi;
+    field_info(c, GS_F_NODE_TAU, fi);
+    const MemberHost& m = c->mem[member];
+    const size_t bytes = 16 * (size_t)m.np;
+    Block k;
+    gs_status st = field_block(c, m, fi, bytes, k);
+    if (st != GS_OK) return st;
+    // the member's own stress (kept for when a storm is switched off), then the live field
+    cudaError_t e = put_block(c, tau_host, bytes, c->d.tau_own, k);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->d.tau + 2 * (size_t)m.np0, c->d.tau_own + 2 * (size_t)m.np0, bytes,
+                            cudaMemcpyDeviceToDevice, c->st);
     return e == cudaSuccess ? GS_OK : c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
 }
 
@@ -1059,7 +1189,13 @@ extern "C" gs_status gs_set_vortex(gs_ctx* c, int member, const gs_vortex* v) {
                                     cudaMemcpyHostToDevice, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
     if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
-    if (!v && was) return gs_set_tau(c, member, c->mem[member].tau.data());   // back to the member's own stress
+    if (!v && was) {
+        // back to the member's own stress
+        const MemberHost& m = c->mem[member];
+        e = cudaMemcpyAsync(c->d.tau + 2 * (size_t)m.np0, c->d.tau_own + 2 * (size_t)m.np0, 16 * (size_t)m.np,
+                            cudaMemcpyDeviceToDevice, c->st);
+        if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    }
     return GS_OK;
 }
 
@@ -1071,9 +1207,10 @@ extern "C" size_t gs_footprint_bytes(int nvrt, int ntr, int nmem, int64_t np, in
     const double L = nvrt, T = ntr;
     const double sell = (double)nnz * 1.25 + 32.0 * kMaxDeg;
     double b = 0.0;
-    b += (double)np * (91.0 + L * (8 + 8 + 16 + 8 * T) + 20.0 + 88.0 + 4.0 * kIrVectors + 4.0 + 332.0);
-    b += (double)ne * (24.0 + 88.0 + 24.0 + 4.0 + 80.0 + L * (24.0 + 16.0 * T));
-    b += (double)ns * (16.0 + 70.0 + 72.0 + 16.0 + 48.0 + L * 52.0);
+    b += (double)np * (91.0 + L * (8 + 8 + 16 + 8 * T) + 20.0 + 88.0 + 4.0 * kIrVectors + 4.0 + 332.0 + 20.0);
+    b += (double)ne * (24.0 + 88.0 + 24.0 + 4.0 + 80.0 + L * (24.0 + 16.0 * T) + 4.0);
+    b += (double)ns * (16.0 + 70.0 + 72.0 + 16.0 + 48.0 + L * 52.0 + 4.0);
+    b += std::max(L * 16.0 * (double)ns, L * 8.0 * T * (double)ne);   // field exchange staging (largest field)
     b += sell * 16.0 + (double)np / 32.0 * 8.0;
     b += ((double)np / 1024.0 + nmem) * 84.0 + (double)nmem * (16.0 + 72.0 + 40.0 + 8.0 * kVortexParams + 64.0);
     b += (double)kMassBlocks * kMaxTracers * 16.0 + kMaxTracers * 8.0;

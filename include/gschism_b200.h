@@ -150,11 +150,30 @@ enum {
     GS_F_CSR_DATA = 40, GS_F_CSR_INDPTR = 41, GS_F_CSR_INDICES = 42, GS_F_JCG_X = 43, GS_F_ELBC = 44,
     GS_F_JCG_X1 = 45, GS_F_JCG_X2 = 46   /* JCG solution history x0 (last), x1, x2 */
 };
-/* bytes must equal the field's size (int32 for *_KB, *_DRY, SIDE_BTELEM, CSR_INDPTR/INDICES). */
+/* bytes must equal the field's size (int32 for *_KB, *_DRY, SIDE_BTELEM, CSR_INDPTR/INDICES).
+ * The numbering permutation runs on the device and a field crosses to the host as one copy
+ * through page-locked staging.  gs_state_get returns when the data is in `host` (it waits for
+ * the work queued before it); gs_state_put copies `host` to staging before it returns (the buffer
+ * may be reused at once) and queues the upload on the context's stream. */
 gs_status gs_state_get(gs_ctx* ctx, int member, int field, void* host, size_t bytes);
 gs_status gs_state_put(gs_ctx* ctx, int member, int field, const void* host, size_t bytes);
-/* Per-step host forcing: replace a member's surface stress [np][2] (host buffer, copied). */
+/* Per-step host forcing: replace a member's surface stress [np][2] (host buffer, copied before
+ * the call returns; the upload is queued on the context's stream, no synchronisation). */
 gs_status gs_set_tau(gs_ctx* ctx, int member, const double* tau_host);
+
+/* Output path (replaces DeviceToHost, src/iop/deviceToHost.py:37-224, the reference's per-field
+ * device-to-host reads for writeOutput, src/iop/writeOutput.py:53-280).
+ * gs_state_get_async queues the read of one field into `host`, which must be page-locked memory
+ * (gs_host_alloc), and returns at once; CSR fields are not available this way.  gs_output_mark
+ * records a point on the context's stream and gs_output_wait blocks the calling host thread until
+ * everything queued before that mark is done (the reads included).  A writer thread can wait
+ * for one record while the stepping thread queues the next steps. */
+gs_status gs_state_get_async(gs_ctx* ctx, int member, int field, void* host, size_t bytes);
+gs_status gs_output_mark(gs_ctx* ctx, uint64_t* ticket);
+gs_status gs_output_wait(gs_ctx* ctx, uint64_t ticket);
+/* Page-locked host memory for gs_state_get_async (NULL on failure) and its release. */
+void* gs_host_alloc(size_t bytes);
+gs_status gs_host_free(void* p);
 
 /* Parametric storm forcing for a member (storm-surge scenarios): a radial vortex moving along a
    straight track, evaluated on the device at the start of every step.  Wind speed at distance r

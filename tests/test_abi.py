@@ -11,7 +11,7 @@ HDR = os.path.join(os.path.dirname(__file__), "..", "include", "gschism_b200.h")
 
 def _declared():
     txt = open(HDR).read()
-    return sorted(set(re.findall(r"^\s*(?:gs_status|const char\*|size_t)\s+(gs_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:gs_status|const char\*|size_t|void\*)\s+(gs_\w+)\s*\(", txt, re.M)))
 
 
 def test_exports_every_declared_symbol(native):
