@@ -134,6 +134,7 @@ struct Dev {
     double *tvds;                  // [ntr][nvrt][NE] TVD inflow sums (allocated with TVD only)
     double *maxDt;
     double2 *ghat;
+    double *rho_n, *rho_e;         // [nvrt][NP], [nvrt][NE] densities (allocated with >= 2 tracers)
     // members
     int32_t *mem_np0, *mem_ne0;    // entity offsets [nmem+1]
     double *vort;                  // [nmem][kVortexParams] storm parameters (gs_vortex + enabled flag)

@@ -2,6 +2,8 @@
 // velocities (meshdata.cu:5765-5929).  The reference accumulates nodal velocities with FP64
 // atomics in thread order; here every node gathers over its counter-clockwise element ball,
 // so the sums are deterministic.
+#include <algorithm>
+
 #include "dev_common.cuh"
 #include "kernels.h"
 
@@ -167,6 +169,41 @@ __global__ void k_nodal_vel(Dev d, Phys P) {
     }
 }
 
+// eqstate, src/kernels/eqstate.h:12-52 (ieos_type = 0, ieos_pres = 0): UNESCO 1980 one-atmosphere
+// density (Millero & Poisson 1981), T and S clamped to their validity range [-2, 40] C, [0, 42] psu
+__device__ __forceinline__ double eqstate(double T, double S) {
+    T = fmax(-2.0, fmin(T, 40.0));
+    S = fmax(0.0, fmin(S, 42.0));
+    const double sqrtS = sqrt(S);
+    const double rhow = 999.842594 + T * (6.793952e-2 + T * (-9.095290e-3 + T * (1.001685e-4
+                        + T * (-1.120083e-6 + T * 6.536332e-9))));
+    const double A = 8.24493e-1 + T * (-4.0899e-3 + T * (7.6438e-5 + T * (-8.2467e-7 + T * 5.3875e-9)));
+    const double B = -5.72466e-3 + T * (1.0227e-4 + T * (-1.6546e-6));
+    return rhow + S * (A + B * sqrtS + 4.8314e-4 * S);
+}
+
+// computeNodeDensity / computeElemDensity, meshdata.cu:6776-6812: density of every (entity, level)
+// from the first two tracers (T, S); -99 on dry entities.  One thread per (entity, level): the
+// tracer slices [t][k][n] are read with unit stride.
+__global__ void k_density(const double* __restrict__ tr, const uint8_t* __restrict__ dry, double* __restrict__ rho,
+                          int n, int nvrt) {
+    const long long total = (long long)n * nvrt;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(g % n);
+        rho[g] = dry[i] ? -99.0 : eqstate(tr[g], tr[total + g]);
+    }
+}
+
+void launch_density(const Dev& d, const Phys& P, cudaStream_t st, int nsm) {
+    if (!d.rho_n || P.ntr < 2) return;
+    const long long tn = (long long)d.NP * P.nvrt, te = (long long)d.NE * P.nvrt;
+    k_density<<<(int)std::min<long long>((tn + 255) / 256, (long long)nsm * 8), 256, 0, st>>>(d.tr, d.ndry, d.rho_n,
+                                                                                            d.NP, P.nvrt);
+    k_density<<<(int)std::min<long long>((te + 255) / 256, (long long)nsm * 8), 256, 0, st>>>(d.etr, d.edry, d.rho_e,
+                                                                                            d.NE, P.nvrt);
+}
+
 void launch_levels(const Dev& d, const Phys& P, const VG& vg, int it, cudaStream_t st, int nsm, const LaunchTable& L) {
     const LaunchShape& s = L.k[LK_LEVELS];
     const int b = s.block;
@@ -176,6 +213,7 @@ void launch_levels(const Dev& d, const Phys& P, const VG& vg, int it, cudaStream
     if (it != 0) k_lev_rewet_nodes<<<grid_of(d.NP, s, nsm), b, 0, st>>>(d, P);
     k_lev_sides<<<grid_of(d.NS, s, nsm), b, 0, st>>>(d, P, it);
     k_lev_sides_dry<<<grid_of(d.NS, s, nsm), b, 0, st>>>(d);
+    launch_density(d, P, st, nsm);
 }
 
 void launch_nodal_vel(const Dev& d, const Phys& P, cudaStream_t st, int nsm, const LaunchTable& L) {

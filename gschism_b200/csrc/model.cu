@@ -573,6 +573,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     AL(ez, (size_t)nvrt * NE); AL(ew, (size_t)nvrt * NE); AL(Qv, (size_t)nvrt * NE);
     UP(etr, B.etr); AL(prev, (size_t)ntr * nvrt * NE);
     if (c->cfg.itr_met == 3) AL(tvds, (size_t)ntr * nvrt * NE); AL(maxDt, NE); AL(ghat, NE);
+    if (ntr >= 2) { AL(rho_n, (size_t)nvrt * NP); AL(rho_e, (size_t)nvrt * NE); }
     UP(mem_np0, B.mem_np0); UP(mem_ne0, B.mem_ne0); UP(elem_member, B.elem_member);
     c->h_vort.assign((size_t)kVortexParams * c->mem.size(), 0.0);
     UP(vort, c->h_vort);
@@ -943,6 +944,8 @@ bool field_info(gs_ctx* c, int f, FieldInfo& fi) {
     case GS_F_ELEM_KB: fi.ent = 'E'; fi.isint = 1; fi.ptr = d.kbe; return true;
     case GS_F_ELEM_DRY: fi.ent = 'E'; fi.isint = 2; fi.ptr = d.edry; return true;
     case GS_F_ELEM_GHAT: fi.ent = 'E'; fi.comp = 2; fi.ptr = d.ghat; return true;
+    case GS_F_NODE_RHO: fi.lev = 1; fi.ptr = d.rho_n; return d.rho_n != nullptr;
+    case GS_F_ELEM_RHO: fi.ent = 'E'; fi.lev = 1; fi.ptr = d.rho_e; return d.rho_e != nullptr;
     case GS_F_CSR_DATA: fi.ent = 'C'; fi.ptr = d.A; return true;
     case GS_F_CSR_INDPTR: fi.ent = 'R'; fi.isint = 1; return true;
     case GS_F_CSR_INDICES: fi.ent = 'C'; fi.isint = 1; return true;
@@ -1207,8 +1210,9 @@ extern "C" size_t gs_footprint_bytes(int nvrt, int ntr, int nmem, int64_t np, in
     const double L = nvrt, T = ntr;
     const double sell = (double)nnz * 1.25 + 32.0 * kMaxDeg;
     double b = 0.0;
-    b += (double)np * (91.0 + L * (8 + 8 + 16 + 8 * T) + 20.0 + 88.0 + 4.0 * kIrVectors + 4.0 + 332.0 + 20.0);
-    b += (double)ne * (24.0 + 88.0 + 24.0 + 4.0 + 80.0 + L * (24.0 + 16.0 * T) + 4.0);
+    const double R = ntr >= 2 ? 8.0 : 0.0;      // densities
+    b += (double)np * (91.0 + L * (8 + 8 + 16 + 8 * T + R) + 20.0 + 88.0 + 4.0 * kIrVectors + 4.0 + 332.0 + 20.0);
+    b += (double)ne * (24.0 + 88.0 + 24.0 + 4.0 + 80.0 + L * (24.0 + 16.0 * T + R) + 4.0);
     b += (double)ns * (16.0 + 70.0 + 72.0 + 16.0 + 48.0 + L * 52.0 + 4.0);
     b += std::max(L * 16.0 * (double)ns, L * 8.0 * T * (double)ne);   // field exchange staging (largest field)
     b += sell * 16.0 + (double)np / 32.0 * 8.0;

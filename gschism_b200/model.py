@@ -23,7 +23,8 @@ FIELDS = dict(ETA1=0, ETA2=1, NODE_Z=2, NODE_U2=3, NODE_W2=4, NODE_TR=5, NODE_KB
               SIDE_U2=10, SIDE_BTU=11, SIDE_ZC=12, SIDE_KB=13, SIDE_DRY=14, SIDE_U=15, SIDE_HHAT=16,
               SIDE_CHI=17, SIDE_QH=18, SIDE_BTELEM=19, SIDE_GRADETA1=20, SIDE_GRADETA2=21,
               ELEM_Z=30, ELEM_W=31, ELEM_QV=32, ELEM_TR=33, ELEM_KB=34, ELEM_DRY=35, ELEM_GHAT=36,
-              CSR_DATA=40, CSR_INDPTR=41, CSR_INDICES=42, JCG_X=43, ELBC=44, JCG_X1=45, JCG_X2=46)
+              CSR_DATA=40, CSR_INDPTR=41, CSR_INDICES=42, JCG_X=43, ELBC=44, JCG_X1=45, JCG_X2=46, NODE_RHO=47,
+              ELEM_RHO=48)
 INT_FIELDS = {"NODE_KB", "NODE_DRY", "SIDE_KB", "SIDE_DRY", "SIDE_BTELEM", "ELEM_KB", "ELEM_DRY",
               "CSR_INDPTR", "CSR_INDICES"}
 
@@ -217,7 +218,7 @@ class Model:
             return (n["N"], 2)
         if name == "ELEM_GHAT":
             return (n["E"], 2)
-        if name in ("NODE_Z", "NODE_W2"):
+        if name in ("NODE_Z", "NODE_W2", "NODE_RHO"):
             return (nv, n["N"])
         if name == "NODE_U2":
             return (nv, n["N"], 2)
@@ -227,7 +228,7 @@ class Model:
             return (nv, n["S"], 2)
         if name in ("SIDE_ZC", "SIDE_QH", "SIDE_BTELEM"):
             return (nv, n["S"])
-        if name in ("ELEM_Z", "ELEM_W", "ELEM_QV"):
+        if name in ("ELEM_Z", "ELEM_W", "ELEM_QV", "ELEM_RHO"):
             return (nv, n["E"])
         if name == "ELEM_TR":
             return (nt, nv, n["E"])

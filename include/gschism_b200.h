@@ -148,7 +148,8 @@ enum {
     GS_F_ELEM_Z = 30, GS_F_ELEM_W = 31, GS_F_ELEM_QV = 32, GS_F_ELEM_TR = 33, GS_F_ELEM_KB = 34,
     GS_F_ELEM_DRY = 35, GS_F_ELEM_GHAT = 36,
     GS_F_CSR_DATA = 40, GS_F_CSR_INDPTR = 41, GS_F_CSR_INDICES = 42, GS_F_JCG_X = 43, GS_F_ELBC = 44,
-    GS_F_JCG_X1 = 45, GS_F_JCG_X2 = 46   /* JCG solution history x0 (last), x1, x2 */
+    GS_F_JCG_X1 = 45, GS_F_JCG_X2 = 46,  /* JCG solution history x0 (last), x1, x2 */
+    GS_F_NODE_RHO = 47, GS_F_ELEM_RHO = 48  /* density [nvrt][n] from tracers 0, 1 (T, S); -99 when dry */
 };
 /* bytes must equal the field's size (int32 for *_KB, *_DRY, SIDE_BTELEM, CSR_INDPTR/INDICES).
  * The numbering permutation runs on the device and a field crosses to the host as one copy

@@ -44,6 +44,8 @@ static void* fptr(const og_model* m, int f, fdesc* d) {
     case OGF_ELEM_KB: d->n = m->ne; d->isint = 1; return m->kbe;
     case OGF_ELEM_DRY: d->n = m->ne; d->isint = 2; return m->edry;
     case OGF_ELEM_GHAT: d->n = m->ne; d->comp = 2; return m->ghat;
+    case OGF_NODE_RHO: d->n = m->np; d->lev = 1; return m->rho_n;
+    case OGF_ELEM_RHO: d->n = m->ne; d->lev = 1; return m->rho_e;
     case OGF_CSR_DATA: d->n = m->nnz; return m->data;
     case OGF_CSR_INDPTR: d->n = m->np + 1; d->isint = 1; return m->indptr;
     case OGF_CSR_INDICES: d->n = m->nnz; d->isint = 1; return m->indices;

@@ -465,6 +465,8 @@ int rd_xfer(int f, void* ext, int to_ext) {
         return 0;
     case 45: SC(NP, m.x1[i])
     case 46: SC(NP, m.x2[i])
+    case 47: LV(NP, nd[i].rho[k])
+    case 48: LV(NE, el[i].rho[k])
     default: return -1;
     }
 #undef SC

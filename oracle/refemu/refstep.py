@@ -35,7 +35,7 @@ FIELDS = dict(ETA1=0, ETA2=1, NODE_Z=2, NODE_U2=3, NODE_W2=4, NODE_TR=5, NODE_KB
               NODE_TAU=9, SIDE_U2=10, SIDE_BTU=11, SIDE_ZC=12, SIDE_KB=13, SIDE_DRY=14, SIDE_U=15,
               SIDE_HHAT=16, SIDE_CHI=17, SIDE_QH=18, SIDE_GRADETA1=20, SIDE_GRADETA2=21, ELEM_Z=30,
               ELEM_W=31, ELEM_QV=32, ELEM_TR=33, ELEM_KB=34, ELEM_DRY=35, ELEM_GHAT=36, CSR_DATA=40,
-              CSR_INDPTR=41, CSR_INDICES=42, JCG_X=43, ELBC=44, JCG_X1=45, JCG_X2=46)
+              CSR_INDPTR=41, CSR_INDICES=42, JCG_X=43, ELBC=44, JCG_X1=45, JCG_X2=46, NODE_RHO=47, ELEM_RHO=48)
 INT_FIELDS = {"NODE_KB", "NODE_DRY", "SIDE_KB", "SIDE_DRY", "ELEM_KB", "ELEM_DRY", "CSR_INDPTR", "CSR_INDICES"}
 
 
@@ -300,7 +300,7 @@ class RefStep:
         nv, nt = self.case.nvrt, self.case.ntracers
         n = {"N": self.np_, "S": self.ns_, "E": self.ne_}[name[0] if name[:4] in ("NODE", "SIDE", "ELEM") else "N"]
         per_level = name in ("NODE_Z", "NODE_U2", "NODE_W2", "SIDE_U2", "SIDE_BTU", "SIDE_ZC", "SIDE_QH",
-                             "ELEM_Z", "ELEM_W", "ELEM_QV")
+                             "ELEM_Z", "ELEM_W", "ELEM_QV", "NODE_RHO", "ELEM_RHO")
         vec = name in ("NODE_U2", "SIDE_U2", "SIDE_BTU", "SIDE_U", "SIDE_GRADETA1", "SIDE_GRADETA2",
                        "ELEM_GHAT", "NODE_TAU")
         if name in ("CSR_DATA", "CSR_INDICES"):

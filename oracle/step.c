@@ -236,6 +236,8 @@ og_model* og_model_create(const og_input* in, int* status) {
     m->maxDt = (double*)xc(ne, 8);
     m->tvds = (double*)xc((size_t)ne * nvrt * (ntr ? ntr : 1), 8);
     m->ghat = (v2*)xc(ne, sizeof(v2));
+    m->rho_n = (double*)xc((size_t)np * nvrt, 8);
+    m->rho_e = (double*)xc((size_t)ne * nvrt, 8);
 
     /* CSR pattern */
     m->nnz = m->nnp_s[np] + np;
@@ -261,7 +263,7 @@ void og_model_free(og_model* m) {
                     m->chi2, m->gE1, m->gE2, m->Qh, m->area, m->edepth, m->gphi, m->ssign, m->kbe,
                     m->edry, m->ez, m->ew, m->Qv, m->etr, m->prev, m->inflow, m->maxDt, m->ghat, m->tvds,
                     m->indptr, m->indices, m->data, m->slot, m->dslot, m->jr, m->jz, m->jp, m->jq,
-                    m->jinvD, m->jb};
+                    m->jinvD, m->jb, m->rho_n, m->rho_e};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(m);
 }
@@ -1000,6 +1002,37 @@ void og_levels(og_model* m, int it) {
         const int wet = !m->edry[e0] || (e1 >= 0 && !m->edry[e1]);
         m->sdry[s] = (uint8_t)!wet;
     }
+    og_density(m);
+}
+
+double og_eqstate(double T, double S) {
+    /* eqstate, eqstate.h:12-52 (ieos_type = 0, ieos_pres = 0): UNESCO 1980 one-atmosphere density
+     * (Millero & Poisson 1981) with T, S clamped to [-2, 40] C and [0, 42] psu */
+    T = fmax(-2.0, fmin(T, 40.0));
+    S = fmax(0.0, fmin(S, 42.0));
+    const double sqrtS = sqrt(S);
+    const double rhow = 999.842594 + T * (6.793952e-2 + T * (-9.095290e-3 + T * (1.001685e-4
+                        + T * (-1.120083e-6 + T * 6.536332e-9))));
+    const double A = 8.24493e-1 + T * (-4.0899e-3 + T * (7.6438e-5 + T * (-8.2467e-7 + T * 5.3875e-9)));
+    const double B = -5.72466e-3 + T * (1.0227e-4 + T * (-1.6546e-6));
+    return rhow + S * (A + B * sqrtS + 4.8314e-4 * S);
+}
+
+void og_density(og_model* m) {
+    /* computeNodeDensity / computeElemDensity, mdc:6776-6812: density per level from the first
+     * two tracers (T, S); dry entities hold -99.  Only with at least two tracers. */
+    if (m->ntr < 2) return;
+    const int nvrt = m->nvrt, ntr = m->ntr;
+    for (int i = 0; i < m->np; i++)
+        for (int k = 0; k < nvrt; k++) {
+            const double* t = &m->tr[((size_t)i * nvrt + k) * ntr];
+            m->rho_n[(size_t)i * nvrt + k] = m->ndry[i] ? -99.0 : og_eqstate(t[0], t[1]);
+        }
+    for (int e = 0; e < m->ne; e++)
+        for (int k = 0; k < nvrt; k++) {
+            const double* t = &m->etr[((size_t)e * nvrt + k) * ntr];
+            m->rho_e[(size_t)e * nvrt + k] = m->edry[e] ? -99.0 : og_eqstate(t[0], t[1]);
+        }
 }
 
 /* ------------------------------------------------------------------ nodal velocities ---- */

@@ -50,7 +50,8 @@ enum {
     OGF_ELEM_Z = 30, OGF_ELEM_W = 31, OGF_ELEM_QV = 32, OGF_ELEM_TR = 33, OGF_ELEM_KB = 34,
     OGF_ELEM_DRY = 35, OGF_ELEM_GHAT = 36,
     OGF_CSR_DATA = 40, OGF_CSR_INDPTR = 41, OGF_CSR_INDICES = 42, OGF_JCG_X = 43,
-    OGF_ELBC = 44, OGF_JCG_X1 = 45, OGF_JCG_X2 = 46
+    OGF_ELBC = 44, OGF_JCG_X1 = 45, OGF_JCG_X2 = 46,
+    OGF_NODE_RHO = 47, OGF_ELEM_RHO = 48
 };
 
 typedef struct og_model og_model;
@@ -77,6 +78,8 @@ void og_vertical_velocity(og_model* m);                        /* mdc:5978-6103 
 int  og_transport(og_model* m, double dt);                     /* step:78-93 */
 void og_levels(og_model* m, int it);                           /* ul0*, mdc:5521-5762 */
 void og_nodal_velocities(og_model* m);                         /* mdc:5765-5929 */
+void og_density(og_model* m);                                  /* mdc:6776-6812 (end of og_levels) */
+double og_eqstate(double T, double S);                         /* eqstate.h:12-52 */
 /* one whole step; returns the JCG iteration count */
 int  og_step(og_model* m, int it);
 /* diagnostics: [0] JCG iterations of the last solve, [1] transport sub-steps of the last

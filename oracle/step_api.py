@@ -17,7 +17,8 @@ F = dict(ETA1=0, ETA2=1, NODE_Z=2, NODE_U2=3, NODE_W2=4, NODE_TR=5, NODE_KB=6, N
          SIDE_U2=10, SIDE_BTU=11, SIDE_ZC=12, SIDE_KB=13, SIDE_DRY=14, SIDE_U=15, SIDE_HHAT=16,
          SIDE_CHI=17, SIDE_QH=18, SIDE_BTELEM=19, SIDE_GRADETA1=20, SIDE_GRADETA2=21,
          ELEM_Z=30, ELEM_W=31, ELEM_QV=32, ELEM_TR=33, ELEM_KB=34, ELEM_DRY=35, ELEM_GHAT=36,
-         CSR_DATA=40, CSR_INDPTR=41, CSR_INDICES=42, JCG_X=43, ELBC=44, JCG_X1=45, JCG_X2=46)
+         CSR_DATA=40, CSR_INDPTR=41, CSR_INDICES=42, JCG_X=43, ELBC=44, JCG_X1=45, JCG_X2=46, NODE_RHO=47,
+         ELEM_RHO=48)
 INT_FIELDS = {"NODE_KB", "NODE_DRY", "SIDE_KB", "SIDE_DRY", "SIDE_BTELEM", "ELEM_KB", "ELEM_DRY",
               "CSR_INDPTR", "CSR_INDICES"}
 
@@ -159,7 +160,7 @@ class OracleModel:
             return (self.np, 2)
         if name == "ELEM_GHAT":
             return (self.ne, 2)
-        if name in ("NODE_Z", "NODE_W2"):
+        if name in ("NODE_Z", "NODE_W2", "NODE_RHO"):
             return (self.nvrt, self.np)
         if name == "NODE_U2":
             return (self.nvrt, self.np, 2)
@@ -169,7 +170,7 @@ class OracleModel:
             return (self.nvrt, self.ns, 2)
         if name in ("SIDE_ZC", "SIDE_QH", "SIDE_BTELEM"):
             return (self.nvrt, self.ns)
-        if name in ("ELEM_Z", "ELEM_W", "ELEM_QV"):
+        if name in ("ELEM_Z", "ELEM_W", "ELEM_QV", "ELEM_RHO"):
             return (self.nvrt, self.ne)
         if name == "ELEM_TR":
             return (self.ntr, self.nvrt, self.ne)

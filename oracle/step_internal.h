@@ -50,6 +50,7 @@ struct og_model {
     double *area, *edepth; v2* gphi; double* ssign;
     int32_t* kbe; uint8_t* edry;
     double *ez, *ew, *Qv, *etr, *prev, *inflow, *maxDt; v2* ghat;
+    double *rho_n, *rho_e;       /* [np*nvrt], [ne*nvrt] densities (ntr >= 2: T and S) */
     double* tvds;                 /* TVD: inflow sum per prism and tracer [ne][nvrt][ntr] */
     int64_t cnt[4];
 };

@@ -23,10 +23,10 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 TRAJ_FACTOR = 10.0
 # floors (relative to the field's largest magnitude) for fields whose envelope is at rounding level
 TRAJ_FLOOR = {"ETA2": 1e-12, "NODE_TR": 1e-12, "ELEM_TR": 1e-12, "SIDE_U2": 1e-11, "NODE_U2": 1e-11,
-              "NODE_W2": 1e-10, "ELEM_W": 1e-10}
+              "NODE_W2": 1e-10, "ELEM_W": 1e-10, "NODE_RHO": 1e-14, "ELEM_RHO": 1e-14}
 # the targets: elevation and tracers 1e-10, velocities (horizontal and vertical) 1e-8 over 100 steps
 TRAJ_CAP = {"ETA2": 1e-10, "NODE_TR": 1e-10, "ELEM_TR": 1e-10, "SIDE_U2": 1e-8, "NODE_U2": 1e-8,
-            "NODE_W2": 1e-7, "ELEM_W": 1e-7}
+            "NODE_W2": 1e-7, "ELEM_W": 1e-7, "NODE_RHO": 1e-12, "ELEM_RHO": 1e-12}
 PHASE_TOL = 1e-12
 PHASE_TOL_FIELD = {"NODE_W2": 1e-11, "ELEM_W": 1e-11, "ELEM_QV": 1e-11}
 

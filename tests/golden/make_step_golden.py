@@ -36,6 +36,7 @@ sys.path.insert(0, ROOT)
 from gschism_b200 import cases  # noqa: E402
 
 SNAP_FIELDS = ("ETA2", "NODE_TR", "ELEM_TR", "SIDE_U2", "NODE_U2", "NODE_W2", "ELEM_W")
+RHO_FIELDS = ("NODE_RHO", "ELEM_RHO")   # cases with T and S (two tracers or more)
 STATE_FIELDS = ("ETA1", "ETA2", "NODE_Z", "NODE_U2", "NODE_W2", "NODE_TR", "NODE_KB", "NODE_DRY", "SIDE_U2",
                 "SIDE_ZC", "SIDE_KB", "SIDE_DRY", "ELEM_Z", "ELEM_TR", "ELEM_KB", "ELEM_DRY", "JCG_X", "JCG_X1",
                 "JCG_X2")
@@ -96,10 +97,15 @@ def _cut(name, a, sub):
     return a[:, idx]
 
 
+def snap_fields(case):
+    return SNAP_FIELDS + (RHO_FIELDS if case.ntracers >= 2 else ())
+
+
 def _run_variant(name, atomic_order, dot_order, fma, out):
     """Child process: one reference run (the mesh is a process-wide global there)."""
     from oracle.refemu.refstep import RefStep
     c, nsteps, snaps, phase_step = step_cases()[name]
+    fields = snap_fields(c)
     sub = subset_indices(c)
     r = RefStep(c, atomic_order=atomic_order, dot_order=dot_order, fma=bool(fma))
     res = {"iters": [], "substeps": []}
@@ -115,7 +121,7 @@ def _run_variant(name, atomic_order, dot_order, fma, out):
                    ("NODAL_VEL", r.nodal_velocities)]
             for ph, fn in seq:
                 fn()
-                for f in PHASE_OUT[ph]:
+                for f in PHASE_OUT[ph] + (RHO_FIELDS if ph == "LEVELS" and c.ntracers >= 2 else ()):
                     res[f"phase_{ph}_{f}"] = r.get(f)
             cnt = r.counts()
         else:
@@ -124,7 +130,7 @@ def _run_variant(name, atomic_order, dot_order, fma, out):
         res["iters"].append(cnt["jcg_iters"])
         res["substeps"].append(cnt["substeps"])
         if it in snaps:
-            for f in SNAP_FIELDS:
+            for f in fields:
                 res[f"snap{it}_{f}"] = _cut(f, r.get(f), sub)
     res["iters"] = np.asarray(res["iters"], np.int32)
     res["substeps"] = np.asarray(res["substeps"], np.int32)
@@ -151,18 +157,19 @@ def make(name):
     c, nsteps, snaps, phase_step = step_cases()[name]
     if phase_step is not None:
         base["phase_step"] = np.int32(phase_step)
-    env = np.zeros((len(snaps), len(SNAP_FIELDS)))
+    fields = snap_fields(c)
+    env = np.zeros((len(snaps), len(fields)))
     for i, s in enumerate(snaps):
-        for j, f in enumerate(SNAP_FIELDS):
+        for j, f in enumerate(fields):
             key = f"snap{s}_{f}"
             env[i, j] = max(_rel(v[key], base[key]) for v in var)
     base["envelope"] = env
-    base["envelope_fields"] = np.array(SNAP_FIELDS)
+    base["envelope_fields"] = np.array(fields)
     base["snap_steps"] = np.asarray(snaps, np.int32)
     base["variant_iters"] = np.stack([v["iters"] for v in var])
     np.savez_compressed(os.path.join(HERE, f"step_{name}.npz"), **base)
     print(name, "steps", nsteps, "iters", base["iters"][:5], "...", "envelope at last snapshot:",
-          {f: f"{env[-1, j]:.1e}" for j, f in enumerate(SNAP_FIELDS)})
+          {f: f"{env[-1, j]:.1e}" for j, f in enumerate(fields)})
 
 
 def main(argv):
