@@ -273,9 +273,11 @@ const char* gs_jcg_last_error(const gs_jcg* s);
  * fixed array inside the library (about 3.1 MiB on every GPU that loads it, kept until the
  * process exits), so n is limited to 65536 rows; larger n returns GS_ERR_ARG.  The first call on
  * a device looks up that array's device address (a one-time set-up per device); that first call
- * should come before any stream capture.  All calls share the array: calls that overlap in time
- * on the GPU (other streams,
- * other host threads) race and must be serialised by the caller.  stream may be NULL. */
+ * should come before any stream capture.  The address is kept for the life of the process, so
+ * the entry point must not be used on a device after that device was reset (cudaDeviceReset or a
+ * reset of its primary context) in the same process.  All calls share the array: calls that
+ * overlap in time on the GPU (other streams, other host threads) race and must be serialised by
+ * the caller.  stream may be NULL. */
 gs_status gs_jcg_solve_csr_noalloc(int n, const int32_t* indptr, const int32_t* indices, const double* data,
                                    const double* b, double* x, double rtol, int maxiter, int check_every,
                                    void* stream, int* iters);
