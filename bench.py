@@ -9,8 +9,9 @@ JCG rtol 1e-12.  Inputs are seeded synthetic data (no dataset involved).
 
 value    = node-level-steps/s of the timed steps (sum of nodes x levels x steps / device time),
            FP32-inner JCG with FP64 refinement ("fp32_ir"), state resident in HBM.
-e2e      = the same loop through the C ABI with host buffers: every step uploads the surface
-           stress field from host memory (gs_set_tau) and reads the elevation back (gs_state_get).
+e2e      = the same loop through the C ABI with page-locked host buffers: every step uploads the
+           surface stress field from host memory (gs_set_tau) and reads the elevation back
+           (gs_state_get).
 roofline = the JCG persistent kernel (dominant), algorithmic bytes per launch / launch time.
 The plain FP64 single-instance form is measured on the same GPU and reported under "fp64".
 ensemble = the batched form: 64 members on meshes of uneven size (20k-500k nodes, 20 levels,
@@ -207,10 +208,12 @@ def run_ours(a):
         res[mode]["jcg_iters_last"] = st["jcg_iters"]
         res[mode]["jcg_outer_last"] = st["jcg_outer"]
         if mode == "fp32_ir":
-            # end-to-end through the C ABI with host buffers: upload tau, step, read eta back
-            tau = np.ascontiguousarray(case.tau.copy())
-            eta = np.zeros(nodes)
+            # end-to-end through the C ABI with page-locked host buffers: upload tau, step, read
+            # eta back
             import ctypes
+            tau_t = torch.from_numpy(np.ascontiguousarray(case.tau)).pin_memory()
+            eta_t = torch.zeros(nodes, dtype=torch.float64).pin_memory()
+            tau, eta = tau_t.numpy(), eta_t.numpy()
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)

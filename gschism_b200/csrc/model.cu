@@ -1023,18 +1023,29 @@ cudaError_t stage(gs_ctx* c, size_t bytes, int& h) {
     return cudaSuccess;
 }
 
-// Host block (reference order) -> device field, stream-ordered: the caller's buffer is copied to
-// pinned staging before the call returns, the upload and the scatter run on the context stream.
+bool page_locked(const void* p) {
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return pa.type == cudaMemoryTypeHost;
+}
+
+// Host block (reference order) -> device field, stream-ordered.  Pageable memory is copied to
+// pinned staging before the call returns; page-locked memory is copied by the DMA engine straight
+// from the caller's buffer and the call returns once that copy is done.  The upload and the
+// scatter run on the context stream either way.
 cudaError_t put_block(gs_ctx* c, const void* host, size_t bytes, void* dst, const Block& k) {
     int h = 0;
     cudaError_t e = stage(c, bytes, h);
     if (e != cudaSuccess) return e;
-    std::memcpy(c->hstage[h], host, bytes);
-    e = cudaMemcpyAsync(c->dstage, c->hstage[h], bytes, cudaMemcpyHostToDevice, c->st);
+    const bool direct = page_locked(host);
+    if (!direct) std::memcpy(c->hstage[h], host, bytes);
+    e = cudaMemcpyAsync(c->dstage, direct ? host : c->hstage[h], bytes, cudaMemcpyHostToDevice, c->st);
     if (e != cudaSuccess) return e;
     cudaEventRecord(c->hev[h], c->st);
     launch_scatter(c->dstage, dst, k.kind, k.n, k.N, k.off, k.nslices, k.nc, k.perm, c->st, c->nsm);
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (e == cudaSuccess && direct) e = cudaEventSynchronize(c->hev[h]);
+    return e;
 }
 
 }  // namespace
@@ -1072,10 +1083,12 @@ extern "C" gs_status gs_state_get(gs_ctx* c, int member, int field, void* host, 
     if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
     launch_gather(fi.ptr, c->dstage, k.kind, k.n, k.N, k.off, k.nslices, k.nc, k.perm,
                   field == GS_F_SIDE_BTELEM ? c->d.pe_ref : nullptr, c->st, c->nsm);
-    e = cudaMemcpyAsync(c->hstage[h], c->dstage, bytes, cudaMemcpyDeviceToHost, c->st);
+    // page-locked destinations take the copy directly, others through pinned staging
+    const bool direct = page_locked(host);
+    e = cudaMemcpyAsync(direct ? host : c->hstage[h], c->dstage, bytes, cudaMemcpyDeviceToHost, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
     if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
-    std::memcpy(host, c->hstage[h], bytes);
+    if (!direct) std::memcpy(host, c->hstage[h], bytes);
     return GS_OK;
 }
 

@@ -155,7 +155,9 @@ enum {
  * The numbering permutation runs on the device and a field crosses to the host as one copy
  * through page-locked staging.  gs_state_get returns when the data is in `host` (it waits for
  * the work queued before it); gs_state_put copies `host` to staging before it returns (the buffer
- * may be reused at once) and queues the upload on the context's stream. */
+ * may be reused at once) and queues the upload on the context's stream.  A page-locked `host`
+ * (gs_host_alloc, cudaHostAlloc) skips the staging copy: the DMA engine reads or writes it
+ * directly, and gs_state_put / gs_set_tau then return once their copy is done. */
 gs_status gs_state_get(gs_ctx* ctx, int member, int field, void* host, size_t bytes);
 gs_status gs_state_put(gs_ctx* ctx, int member, int field, const void* host, size_t bytes);
 /* Per-step host forcing: replace a member's surface stress [np][2] (host buffer, copied before

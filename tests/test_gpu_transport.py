@@ -75,12 +75,15 @@ def test_tvd_without_limiter_is_upwind_on_gpu(native):
     assert np.array_equal(up.get(0, "NODE_TR"), tv.get(0, "NODE_TR"))
 
 
-def test_transport_stress_matches_oracle(native, oracle_lib):
+@pytest.mark.parametrize("n", [60, 200])
+def test_transport_stress_matches_oracle(native, oracle_lib, n):
     """Closed basin, 40 levels, 5 tracers with fronts and blobs, wind-driven, TVD (van Leer) with
-    vertical diffusion: GPU vs oracle over 10 steps, tracer bounds and the mass budget."""
+    vertical diffusion: GPU vs oracle over 10 steps, tracer bounds and the mass budget; n x n nodes
+    (200 x 200: 40,000 nodes, 1.6M prisms per tracer), the transport-stress configuration's layout
+    at a size the oracle steps in seconds."""
     from gschism_b200.model import Model
     from oracle.step_api import OracleModel
-    c = cases.transport_stress(n=60, nsteps=10)
+    c = cases.transport_stress(n=n, nsteps=10)
     o = OracleModel(c)
     g = Model([c])
     tr0 = o.get("ELEM_TR")
