@@ -214,14 +214,21 @@ def run_ours(a):
             tau_t = torch.from_numpy(np.ascontiguousarray(case.tau)).pin_memory()
             eta_t = torch.zeros(nodes, dtype=torch.float64).pin_memory()
             tau, eta = tau_t.numpy(), eta_t.numpy()
+
+            def e2e_step():
+                m.set_tau(0, tau)
+                m.step(1)
+                m.lib.gs_state_get(m.h, 0, 1, eta.ctypes.data_as(ctypes.c_void_p), eta.nbytes)
+
+            # untimed warm-up of this path: its first gs_step captures the step graph
+            for _ in range(max(1, min(a.warmup, 3))):
+                e2e_step()
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             t0 = time.perf_counter()
             for k in range(a.steps):
-                m.set_tau(0, tau)
-                m.step(1)
-                m.lib.gs_state_get(m.h, 0, 1, eta.ctypes.data_as(ctypes.c_void_p), eta.nbytes)
+                e2e_step()
             e1.record(stream)
             torch.cuda.synchronize()
             wall = time.perf_counter() - t0

@@ -61,12 +61,6 @@ struct JcgTiling {
     int tiles = 592;        // tiles of a large member (one per block of a 4-blocks-per-SM grid)
     int min_rows = 1024;    // smallest tile (four rows per thread of a 256-thread block)
     int per_sm = 4;         // cap of the cooperative grid in blocks per SM
-    // several members: deal each member's tiles to the blocks in runs of this many tiles (every
-    // block holds a share of every large member); 0: contiguous tile ranges per block
-#ifndef GS_JCG_INTERLEAVE_DEFAULT
-#define GS_JCG_INTERLEAVE_DEFAULT 0
-#endif
-    int interleave = GS_JCG_INTERLEAVE_DEFAULT;
 };
 struct LaunchTable {
     LaunchShape k[LK_COUNT] = {{128, 32}, {256, 16}, {256, 16}, {128, 16}, {128, 32},

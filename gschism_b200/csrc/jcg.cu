@@ -41,7 +41,6 @@ struct JcgView {
     float* ir32;                   // kIrVectors FP32 vectors of the refinement solve
     const float* diag32;           // D in FP32
     const int32_t *tile_r0, *tile_r1, *tile_mem, *mem_t0, *mem_t1, *blk_t0;   // blk_t0: [grid+1]
-    const int32_t* blk_tiles;      // tile of each slot of blk_t0's ranges (null: slot j is tile j)
     double* tile_part;             // [R_KINDS][ntiles]
     double* mem_atol2;             // [nmem]
     int32_t* mdone;                // [nmem] iterations at convergence, -1 while active
@@ -169,15 +168,10 @@ __device__ __forceinline__ bool checkpoint(const JcgView& J, int it, int maxit) 
     return ((it + 1) % J.check_every == 0) || (it == maxit - 1);
 }
 
-// The tile in slot j of this block's range (blocks may hold tiles of several members in a
-// fixed member order: see block_slots)
-__device__ __forceinline__ int tile_at(const JcgView& J, int j) { return J.blk_tiles ? J.blk_tiles[j] : j; }
-
 // |b|^2 partials (and zero the search directions of both precisions)
 __device__ void phase_bb(const JcgView& J, double* sh) {
     const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
-    for (int j = tb0; j < tb1; j++) {
-        const int t = tile_at(J, j);
+    for (int t = tb0; t < tb1; t++) {
         const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
         double v[1] = {0.0};
         for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
@@ -193,8 +187,7 @@ __device__ void phase_bb(const JcgView& J, double* sh) {
 // atol^2 per member (owner = block holding the member's first tile); atol = 0 retires it
 __device__ void phase_atol(const JcgView& J, double* sh) {
     const int tb0 = J.blk_t0[blockIdx.x], tb1 = J.blk_t0[blockIdx.x + 1];
-    for (int j = tb0; j < tb1; j++) {
-        const int t = tile_at(J, j);
+    for (int t = tb0; t < tb1; t++) {
         const int m = J.tile_mem[t];
         if (t != J.mem_t0[m]) continue;
         const int kinds[1] = {R_BB};
@@ -318,8 +311,7 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
     {
         int cm = -1;
         bool on = false;
-        for (int j = tb0; j < tb1; j++) {
-        const int t = tile_at(J, j);
+        for (int t = tb0; t < tb1; t++) {
             const int m = J.tile_mem[t];
             if (m != cm) {
                 if (cm >= 0 && on && arrive64(J, cm, &shv) && tid == 0) publish64(J, cm, 1, 1, 0.0);
@@ -353,8 +345,7 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
             int cm = -1;
             bool on = false;
             double beta = 0.0;
-            for (int j = tb0; j < tb1; j++) {
-        const int t = tile_at(J, j);
+            for (int t = tb0; t < tb1; t++) {
                 const int m = J.tile_mem[t];
                 if (m != cm) {
                     if (cm >= 0 && on && arrive64(J, cm, &shv)) {
@@ -402,8 +393,7 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
             int cm = -1;
             bool on = false;
             double alpha = 0.0;
-            for (int j = tb0; j < tb1; j++) {
-        const int t = tile_at(J, j);
+            for (int t = tb0; t < tb1; t++) {
                 const int m = J.tile_mem[t];
                 if (m != cm) {
                     if (cm >= 0 && on && arrive64(J, cm, &shv)) publish_beta(J, cm, it + 1, sh);
@@ -582,8 +572,7 @@ __global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgVi
         // sweep starts from p = s~ = 0); outer r.r partials
         {
             float4* uw0 = ir_uws(J, 0);
-            for (int j = tb0; j < tb1; j++) {
-        const int t = tile_at(J, j);
+            for (int t = tb0; t < tb1; t++) {
                 const int m = J.tile_mem[t];
                 const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
                 const int dn = uniform_ld(&J.mdone[m], &shv);
@@ -619,8 +608,7 @@ __global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgVi
         {
             float4* uw0 = ir_uws(J, 0);
             const float* u0 = J.ir32;          // u components of parity 0 (stride 4)
-            for (int j = tb0; j < tb1; j++) {
-        const int t = tile_at(J, j);
+            for (int t = tb0; t < tb1; t++) {
                 const int m = J.tile_mem[t];
                 if (uniform_ld(&J.mdone[m], &shv) >= 0) continue;
                 const int kinds1[1] = {R_OUT};
@@ -670,8 +658,7 @@ __global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgVi
             int cm = -1;
             bool on = false;
             float al = 0.0f, bt = 0.0f;
-            for (int j = tb0; j < tb1; j++) {
-        const int t = tile_at(J, j);
+            for (int t = tb0; t < tb1; t++) {
                 const int m = J.tile_mem[t];
                 if (m != cm) {
                     if (cm >= 0 && on) member_arrive(J, cm, it, np, sh, &shv);
@@ -735,8 +722,7 @@ __global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgVi
         }
         // x += d for the members of this sweep; the sweep's owner closes the member's count
         // (members still on at the iteration cap count it in full)
-        for (int j = tb0; j < tb1; j++) {
-        const int t = tile_at(J, j);
+        for (int t = tb0; t < tb1; t++) {
             const int m = J.tile_mem[t];
             if (uniform_ld(&J.mdone[m], &shv) >= 0) continue;
             const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
@@ -745,8 +731,7 @@ __global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgVi
         }
         GSYNC();
     }
-    for (int j = tb0; j < tb1; j++) {
-        const int t = tile_at(J, j);
+    for (int t = tb0; t < tb1; t++) {
         const int m = J.tile_mem[t];
         if (t == J.mem_t0[m] && tid == 0 && ld_done(J, m) < 0) {
             J.mdone[m] = J.minner[m];
@@ -762,7 +747,6 @@ struct JcgWork {
     bool sell = false;               // kernels instantiated for the SELL-32 layout
     int32_t *tile_r0 = nullptr, *tile_r1 = nullptr, *tile_mem = nullptr, *mem_t0 = nullptr, *mem_t1 = nullptr;
     int32_t *blk64 = nullptr, *blkir = nullptr;
-    int32_t *slot64 = nullptr, *slotir = nullptr;   // tile of every block slot (null: slot = tile)
     double *tile_part = nullptr, *mem_atol2 = nullptr, *mem_ab = nullptr;
     // per-member control words in one array: mdone, mouter, minner, mret, mgen, mcnt ([nmem] each),
     // ndone, status (ERR_JCG_NOT_CONVERGED of the last solve)
@@ -801,36 +785,6 @@ static void block_ranges(const std::vector<int32_t>& tr0, const std::vector<int3
     }
 }
 
-// Block slots of a batch: every block takes a share of every member large enough to span several
-// blocks, and all blocks visit the members in the same order.  Member m's tiles are dealt to the
-// blocks in runs of `chunk` consecutive tiles, round-robin from where the previous member's
-// dealing stopped, so each block holds about the same number of tiles.  With the member-level
-// synchronisation of the solves, a block that has finished its tiles of member m goes on with its
-// tiles of the next members instead of waiting for m's scalars: by the time it comes back to m in
-// the next iteration the other blocks have long published them.  A member's tiles, their rows and
-// the order its partial sums are added in do not change (tile order), so results are the same bits
-// as with contiguous ranges.  Returns the per-block slot ranges bt[grid+1] and the slot list.
-static void block_slots(const std::vector<int32_t>& tm, int nmem, int grid, int chunk, std::vector<int32_t>& bt,
-                        std::vector<int32_t>& slots) {
-    const int T = (int)tm.size();
-    std::vector<std::vector<int32_t>> per(grid);
-    int b = 0, run = 0;
-    for (int t = 0; t < T; t++) {
-        per[b].push_back(t);
-        if (++run == chunk || t + 1 == T || tm[t + 1] != tm[t]) {
-            run = 0;
-            b = (b + 1) % grid;
-        }
-    }
-    (void)nmem;
-    bt.assign(grid + 1, 0);
-    slots.clear();
-    for (int k = 0; k < grid; k++) {
-        slots.insert(slots.end(), per[k].begin(), per[k].end());
-        bt[k + 1] = (int32_t)slots.size();
-    }
-}
-
 static int coop_blocks(const void* fn, int nsm, int cap = 4) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0);
@@ -865,21 +819,14 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     w->sell = sell;
     w->grid64 = std::max(1, std::min(T, coop_blocks(f64, nsm, tiling.per_sm)));
     w->gridir = std::max(1, std::min(T, coop_blocks(fir, nsm, tiling.per_sm)));
-    std::vector<int32_t> b64, bir, s64, sir;
-    const bool deal = tiling.interleave > 0 && nmem > 1;
-    if (deal) {
-        block_slots(tm, nmem, w->grid64, tiling.interleave, b64, s64);
-        block_slots(tm, nmem, w->gridir, tiling.interleave, bir, sir);
-    } else {
-        block_ranges(tr0, tr1, w->grid64, b64);
-        block_ranges(tr0, tr1, w->gridir, bir);
-    }
+    std::vector<int32_t> b64, bir;
+    block_ranges(tr0, tr1, w->grid64, b64);
+    block_ranges(tr0, tr1, w->gridir, bir);
     cudaError_t e = cudaSuccess;
     auto A = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes ? bytes : 8); };
     A((void**)&w->tile_r0, 4 * T); A((void**)&w->tile_r1, 4 * T); A((void**)&w->tile_mem, 4 * T);
     A((void**)&w->mem_t0, 4 * nmem); A((void**)&w->mem_t1, 4 * nmem);
     A((void**)&w->blk64, 4 * b64.size()); A((void**)&w->blkir, 4 * bir.size());
-    if (deal) { A((void**)&w->slot64, 4 * s64.size()); A((void**)&w->slotir, 4 * sir.size()); }
     A((void**)&w->tile_part, 8 * (size_t)R_KINDS * T);
     A((void**)&w->mem_atol2, 16 * (size_t)nmem);
     A((void**)&w->mem_ab, 72 * (size_t)nmem);
@@ -893,19 +840,17 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     w->status = w->mctl + 6 * nmem + 1;
     {
         // blocks of each grid holding tiles of each member
-        auto count = [&](const std::vector<int32_t>& bt, const std::vector<int32_t>& sl, int grid, int32_t* dst) {
+        auto count = [&](const std::vector<int32_t>& bt, int grid, int32_t* dst) {
             std::vector<int32_t> nb(nmem, 0);
             for (int b = 0; b < grid; b++) {
                 int last = -1;
-                for (int j = bt[b]; j < bt[b + 1]; j++) {
-                    const int t = sl.empty() ? j : sl[j];
+                for (int t = bt[b]; t < bt[b + 1]; t++)
                     if (tm[t] != last) { last = tm[t]; nb[last]++; }
-                }
             }
             cudaMemcpyAsync(dst, nb.data(), 4 * (size_t)nmem, cudaMemcpyHostToDevice, st);
         };
-        count(bir, sir, w->gridir, w->mnblk);
-        count(b64, s64, w->grid64, w->mnblk64);
+        count(bir, w->gridir, w->mnblk);
+        count(b64, w->grid64, w->mnblk64);
     }
     // uploads on the caller's stream, never the legacy default stream (pageable sources are
     // staged before each call returns)
@@ -916,10 +861,6 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     cudaMemcpyAsync(w->mem_t1, mt1.data(), 4 * nmem, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(w->blk64, b64.data(), 4 * b64.size(), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(w->blkir, bir.data(), 4 * bir.size(), cudaMemcpyHostToDevice, st);
-    if (deal) {
-        cudaMemcpyAsync(w->slot64, s64.data(), 4 * s64.size(), cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(w->slotir, sir.data(), 4 * sir.size(), cudaMemcpyHostToDevice, st);
-    }
     cudaMemsetAsync(w->tile_part, 0, 8 * (size_t)R_KINDS * T, st);
     cudaMemsetAsync(w->mctl, 0, 4 * (6 * (size_t)nmem + 2), st);
     cudaStreamSynchronize(st);
@@ -928,7 +869,7 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
 
 void jcg_work_free(JcgWork* w) {
     if (!w) return;
-    void* ps[] = {w->tile_r0, w->tile_r1, w->tile_mem, w->mem_t0, w->mem_t1, w->blk64, w->blkir, w->slot64, w->slotir,
+    void* ps[] = {w->tile_r0, w->tile_r1, w->tile_mem, w->mem_t0, w->mem_t1, w->blk64, w->blkir,
                   w->tile_part, w->mem_atol2, w->mem_ab, w->mctl, w->mnblk, w->mnblk64};
     for (void* p : ps) cudaFree(p);
     delete w;
@@ -945,7 +886,6 @@ cudaError_t jcg_launch(const JcgArgs& a, JcgWork* w, cudaStream_t st, int nsm) {
     J.mem_t0 = w->mem_t0; J.mem_t1 = w->mem_t1;
     const bool ir = (a.precision == GS_FP32_IR);
     J.blk_t0 = ir ? w->blkir : w->blk64;
-    J.blk_tiles = ir ? w->slotir : w->slot64;
     J.tile_part = w->tile_part; J.mem_atol2 = w->mem_atol2;
     J.mdone = w->mdone; J.mouter = w->mouter; J.minner = w->minner; J.mret = w->mret; J.ndone = w->ndone;
     J.mem_ab = w->mem_ab; J.mpub = w->mem_ab + 4 * (size_t)w->nmem;
@@ -1083,7 +1023,6 @@ extern "C" gs_status gs_jcg_solve_csr_noalloc(int n, const int32_t* indptr, cons
     J.tile_r1 = J.tile_r0 + kNoAllocMaxTiles;
     J.tile_mem = J.tile_r1 + kNoAllocMaxTiles;
     J.blk_t0 = (const int32_t*)(base + kNaOffBlk);
-    J.blk_tiles = nullptr;
     J.mem_t0 = ctl + 0; J.mem_t1 = ctl + 1; J.mdone = ctl + 2; J.mouter = ctl + 3;
     J.ndone = (unsigned*)(ctl + 4); J.bar = (unsigned*)(ctl + 5);
     J.err = ctl + 7; J.status = ctl + 6;
