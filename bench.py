@@ -267,7 +267,10 @@ def run_ours(a):
                                  else JCG_DRAM_BYTES_PER_INNER_ITER * it_in), "kernel": "k_jcg_ir",
                      "peak_kind": peak_kind, "iters_per_launch": it_in, "bytes_per_launch": bytes_launch},
         "clocks": r["clocks"],
-        "gpu_launches": a.steps * 18,
+        # per step, issued phase by phase: clock, btrack, elevation BC, side preparation, ghat, assembly,
+        # solve, elevation update, momentum, vertical velocity, transport, nodal tracers, 6 level kernels,
+        # 2 density kernels (two tracers), nodal velocities (the launch list in profiles/)
+        "gpu_launches": a.steps * 22,
         "jcg": {"inner_iters": r["jcg_iters_last"], "outer": r["jcg_outer_last"], "ms_avg": jms_avg},
     }
     if "fp64" in res:
