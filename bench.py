@@ -138,7 +138,7 @@ class Clocks:
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per inner iteration of k_jcg_ir on
 # the 1M-node basin, from the ncu capture summarised in profiles/k_jcg_ir_basin1M.md (launch
 # bytes / inner iterations of that launch); scaled here by the timed launches' inner iterations.
-JCG_DRAM_BYTES_PER_INNER_ITER = 31.6e6
+JCG_DRAM_BYTES_PER_INNER_ITER = 18.7e6
 
 
 def _jcg_bytes_per_iter(N, nnz, mode):
