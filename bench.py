@@ -24,7 +24,8 @@ cpu_baseline = the oracle on the benchmarked mesh itself (all host threads), 2 t
 --impl reference = the same oracle on the benchmarked mesh, 1 warm-up + up to 6 timed steps (a
            bounded sample of the run), plus a single-thread figure on a 200 x 200 sample.
 Multi-GPU (torchrun): every rank steps its own replica of the mesh (no data exchange exists in
-the step); value = all ranks' node-level-steps / the max over ranks of the device time.
+the step); value = all ranks' node-level-steps / the max over ranks of the device time.  The
+64-member ensemble is then sharded over the ranks by device footprint (`ensemble_sharded`).
 """
 from __future__ import annotations
 
@@ -237,6 +238,9 @@ def run_ours(a):
                                     h2d_bytes_per_step=int(tau.nbytes), d2h_bytes_per_step=int(eta.nbytes))
         m.close()
         del m
+    # several GPUs: the 64-member ensemble sharded by device footprint (every rank steps its own
+    # members; the device time is the max over ranks)
+    ens_sharded = run_ensemble_sharded(a, stream, local, dist, ws, rank) if (ws > 1 and not a.no_ensemble) else None
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
@@ -279,6 +283,8 @@ def run_ours(a):
                         "jcg_ms_avg": statistics.mean(f["jcg_ms"])}
     if ens is not None:
         line["ensemble"] = ens
+    if ens_sharded is not None:
+        line["ensemble_sharded"] = ens_sharded
     if srv is not None:
         line["serving"] = srv
     if not a.no_cpu:
@@ -385,6 +391,42 @@ def run_ensemble(a, stream, local):
                                    "note": "members stepped one at a time, sum of their device times"}
     out["speedup_fp32_ir_batched_vs_fp64_single"] = tot / out["fp32_ir_batched"]["ms_per_step"]
     return out
+
+
+def run_ensemble_sharded(a, stream, local, dist, ws, rank):
+    """The 64-member ensemble over `ws` ranks (gschism_b200/shard.py): members assigned by device
+    footprint, each rank steps its share batched (FP32+IR), device time max over ranks.  Every rank
+    takes the same collective steps (a barrier, one max)."""
+    import torch
+    from gschism_b200 import cases
+    from gschism_b200.model import Model, footprint_bytes
+    from gschism_b200.shard import max_over_ranks, shard_members
+    ens = cases.ensemble(n_members=64)
+    mine = shard_members([footprint_bytes([c]) for c in ens], ws)[rank]
+    steps, warm = min(a.steps, 5), 3
+    m = Model([ens[i] for i in mine], precision="fp32_ir", device=local) if mine else None
+    if m is not None:
+        m.set_stream(stream.cuda_stream)
+        for _ in range(warm):
+            m.step(1)
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    if m is not None:
+        for _ in range(steps):
+            m.step(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, device="cuda")
+    if m is not None:
+        m.close()
+    nodes = sum(c.n_nodes for c in ens)
+    nvrt = ens[0].vgrid.nvrt
+    return {"workload": f"the 64-member ensemble ({nodes} nodes, {nvrt} levels) sharded over {ws} GPUs by device footprint",
+            "value": nodes * nvrt * steps / (ms / 1e3), "unit": METRIC, "ms_per_step": ms / steps, "steps": steps,
+            "warmup": warm, "scaling": "strong", "members_on_rank0": len(mine) if rank == 0 else None}
 
 
 def run_serving(local, n=8, rate=2.0, hours=6.0, seed=1):
