@@ -50,7 +50,7 @@ class Params:
     rtol: float = 1e-12              # JCG relative tolerance
     maxiter: int = 1500              # JCG iteration cap
     check_every: int = 10            # JCG host/device convergence test period
-    itr_met: int = 1                 # tracer transport: 1 upwind (the reference), 3 TVD
+    itr_met: int = 1                 # tracer transport: 1 upwind (the reference), 3 TVD, 4 TVD + vertical FCT
     tvd_limiter: int = 3             # TVD flux limiter: 0 none, 1 minmod, 2 Osher, 3 van Leer, 4 superbee
     dfh0: float = 0.0                # constant vertical tracer diffusivity [m^2/s] (implicit)
 

@@ -75,6 +75,7 @@ struct Phys {
     double dt, thetai, h0, dtb_min, dtb_max, velmin, rmaxvel, dfv0, coricoef, rho0, grav, dramp;
     int ihhat;
     int tvd, tvd_limiter;          // TVD horizontal transport and its limiter (0 none .. 4 superbee)
+    int tvd_vert;                  // flux-corrected vertical step (itr_met = 4)
     double dfh0;                   // constant vertical tracer diffusivity (implicit; 0 = none)
 };
 
@@ -132,6 +133,7 @@ struct Dev {
     double *ez, *ew, *Qv;          // [nvrt][NE]
     double *etr, *prev;            // [ntr][nvrt][NE]
     double *tvds;                  // [ntr][nvrt][NE] TVD inflow sums (allocated with TVD only)
+    double *vgam;                  // [nvrt][NE] vertical sweep scratch (allocated with vertical FCT only)
     double *maxDt;
     double2 *ghat;
     double *rho_n, *rho_e;         // [nvrt][NP], [nvrt][NE] densities (allocated with >= 2 tracers)

@@ -26,6 +26,18 @@
 // (psi = 0) reproduces the upwind scheme bit for bit.  The vertical solve optionally adds a
 // constant diffusivity between prism centres.  This file is compiled with -fmad=false so that
 // the limiter's branches see the same rounding as the FP64 CPU restatement.
+//
+// Vertical FCT (itr_met = 4: the TVD horizontal passes plus a flux-corrected vertical step; no
+// counterpart in the reference either): Zalesak's (1979) flux-corrected transport with the
+// implicit upwind solve as the low-order scheme.  After the Thomas sweep gives C^L, interior
+// interface j of a column carries the anti-diffusive transfer a_j = dt |Qv| (C^L_{j+1} - C^L_j)/2
+// (central minus upwind flux), scaled by min(R+ of the receiver, R- of the giver), R+/- =
+// min(1, Q+/-/P+/-) from the prism's incoming / outgoing transfers P and its room to the bounds Q
+// = V (C_max/min - C^L) over the prism and its column neighbours, of C^L and of the field before
+// the vertical step.  The transfers are antisymmetric, so the column's tracer mass is unchanged,
+// and no new extremum appears whatever the vertical Courant number.  The field before the step is
+// kept in prev (copied there by the forward sweep when the horizontal result sits in etr) and
+// the sweep's eliminated super-diagonal goes to its own column scratch.
 #include "dev_common.cuh"
 #include "kernels.h"
 
@@ -116,11 +128,59 @@ __device__ __forceinline__ ElemSides elem_sides(const Dev& d, int e) {
     return q;
 }
 
+// Flux-corrected vertical step of element e's column (FCT above): dst holds C^L and co the field
+// before the vertical step; streamed from the bed up with a window of three prisms, each prism's
+// corrected value written two levels behind the read.  The expression order is the CPU
+// restatement's.
+template <int NTR>
+__device__ void vertical_fct(const Dev& d, const Phys& P, int e, double dt, const double* co_all, double* dst) {
+    const int NE = d.NE, nvrt = P.nvrt;
+    const size_t trs = (size_t)nvrt * NE;
+    const int k0 = d.kbe[e] + 1;
+    const int n = nvrt - k0;
+    if (n < 2) return;
+#pragma unroll 1
+    for (int t = 0; t < NTR; t++) {
+        const double* co = co_all + t * trs;
+        double* cl = dst + t * trs;
+        // prisms i-2 (m2) and i-1 (m1); raw transfer of face (i-2, i-1); scaled transfer of face
+        // (i-3, i-2); limiter factors of prism i-2
+        double cl_m2 = 0.0, cl_m1 = 0.0, co_m2 = 0.0, co_m1 = 0.0, v_m2 = 1.0, v_m1 = 1.0;
+        double a_m2 = 0.0, fa_m3 = 0.0, rp_m2 = 1.0, rm_m2 = 1.0;
+        for (int i = 0; i <= n + 1; i++) {
+            double cl_i = 0.0, co_i = 0.0, v_i = 1.0, a_m1 = 0.0;
+            if (i < n) {
+                const size_t ix = (size_t)(k0 + i) * NE + e;
+                cl_i = cl[ix]; co_i = co[ix]; v_i = evol(d, e, k0 + i - 1);
+                if (i >= 1) a_m1 = 0.5 * dt * fabs(d.Qv[(size_t)(k0 + i - 1) * NE + e]) * (cl_i - cl_m1);
+            }
+            double rp_m1 = 1.0, rm_m1 = 1.0, fa_m2 = 0.0;
+            if (i >= 1 && i <= n) {
+                // limiter factors of prism i-1: transfers a_m2 (below) and a_m1 (above)
+                double cmax = fmax(cl_m1, co_m1), cmin = fmin(cl_m1, co_m1);
+                if (i >= 2) { cmax = fmax(cmax, fmax(cl_m2, co_m2)); cmin = fmin(cmin, fmin(cl_m2, co_m2)); }
+                if (i < n) { cmax = fmax(cmax, fmax(cl_i, co_i)); cmin = fmin(cmin, fmin(cl_i, co_i)); }
+                const double pp = fmax(0.0, a_m2) + fmax(0.0, -a_m1);
+                const double pm = fmin(0.0, a_m2) + fmin(0.0, -a_m1);
+                const double qp = v_m1 * (cmax - cl_m1), qm = v_m1 * (cmin - cl_m1);
+                rp_m1 = pp > 0.0 ? fmin(1.0, qp / pp) : 1.0;
+                rm_m1 = pm < 0.0 ? fmin(1.0, qm / pm) : 1.0;
+                if (i >= 2) fa_m2 = a_m2 * (a_m2 > 0.0 ? fmin(rp_m1, rm_m2) : fmin(rm_m1, rp_m2));
+            }
+            if (i >= 2) cl[(size_t)(k0 + i - 2) * NE + e] = cl_m2 + (fa_m3 - fa_m2) / v_m2;
+            fa_m3 = fa_m2; a_m2 = a_m1; rp_m2 = rp_m1; rm_m2 = rm_m1;
+            cl_m2 = cl_m1; co_m2 = co_m1; v_m2 = v_m1;
+            cl_m1 = cl_i; co_m1 = co_i; v_m1 = v_i;
+        }
+    }
+}
+
 // verticalAdvectionUpdate, meshdata.cu:6611-6665 (upwind: phi = 0) for the NTR tracers of
 // element e: reads the column from src, writes it to dst (src may equal dst), uses scr (one
 // level-major slice) for the eliminated super-diagonal.  Same arithmetic as the reference's
-// tridag_sch<1> (meshdata.cu:3664-3716) row by row.
-template <int NTR>
+// tridag_sch<1> (meshdata.cu:3664-3716) row by row; with FCT, scr is the column scratch and the
+// flux correction follows.
+template <int NTR, bool FCT>
 __device__ void vertical_upwind(const Dev& d, const Phys& P, int e, double dt, const double* src, double* dst,
                                 double* scr) {
     const int NE = d.NE, nvrt = P.nvrt;
@@ -157,7 +217,9 @@ __device__ void vertical_upwind(const Dev& d, const Phys& P, int e, double dt, c
             bet = bdia;
 #pragma unroll
             for (int t = 0; t < NTR; t++) {
-                up[t] = (src[t * trs + ix] * 1.0) / bet;
+                const double c = src[t * trs + ix];
+                if (FCT && src == dst) d.prev[t * trs + ix] = c;   // keep the field before the step
+                up[t] = (c * 1.0) / bet;
                 dst[t * trs + ix] = up[t];
             }
         } else {
@@ -165,7 +227,9 @@ __device__ void vertical_upwind(const Dev& d, const Phys& P, int e, double dt, c
             bet = bdia - alow * gam;
 #pragma unroll
             for (int t = 0; t < NTR; t++) {
-                up[t] = (src[t * trs + ix] * 1.0 - alow * up[t]) / bet;
+                const double c = src[t * trs + ix];
+                if (FCT && src == dst) d.prev[t * trs + ix] = c;
+                up[t] = (c * 1.0 - alow * up[t]) / bet;
                 dst[t * trs + ix] = up[t];
             }
             scr[ix] = gam;           // after the reads: scr may be src's first tracer slice
@@ -182,13 +246,18 @@ __device__ void vertical_upwind(const Dev& d, const Phys& P, int e, double dt, c
             dst[t * trs + ix] = up[t];
         }
     }
+    if (FCT) {
+        vertical_fct<NTR>(d, P, e, dt, d.prev, dst);
+#pragma unroll
+        for (int t = 0; t < NTR; t++) up[t] = dst[t * trs + (size_t)k0 * NE + e];
+    }
     // levels at and below the bed take the bottom prism's value
     for (int k = 0; k <= kb; k++)
 #pragma unroll
         for (int t = 0; t < NTR; t++) dst[t * trs + (size_t)k * NE + e] = up[t];
 }
 
-template <int NTR, bool TVD>
+template <int NTR, bool TVD, bool FCT>
 __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
     const int NE = d.NE, NS = d.NS, nvrt = P.nvrt, nmem = d.nmem;
     const size_t trs = (size_t)nvrt * NE;
@@ -412,7 +481,7 @@ __global__ void __launch_bounds__(256) k_transport(Dev d, Phys P, TrArgs T) {
         if (d.edry[e]) continue;
         const int m = d.elem_member[e];
         const double* res = (T.nsub[m] & 1) ? d.prev : d.etr;
-        vertical_upwind<NTR>(d, P, e, T.dt, res, d.etr, d.prev);
+        vertical_upwind<NTR, FCT>(d, P, e, T.dt, res, d.etr, FCT ? d.vgam : d.prev);
     }
 }
 
@@ -519,7 +588,9 @@ template <int NTR>
 static cudaError_t launch_ntr(const Dev& d, const Phys& P, TrArgs& T, cudaStream_t st, int nsm, const LaunchShape& nt) {
     // the TVD passes live in their own instantiation, so the upwind one keeps its smaller
     // register budget and its occupancy
-    const void* fn = P.tvd ? (const void*)k_transport<NTR, true> : (const void*)k_transport<NTR, false>;
+    const void* fn = P.tvd_vert ? (const void*)k_transport<NTR, true, true>
+                     : P.tvd    ? (const void*)k_transport<NTR, true, false>
+                                : (const void*)k_transport<NTR, false, false>;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0);
     if (per_sm < 1) per_sm = 1;

@@ -159,7 +159,7 @@ gs_status gs_ctx_create(const gs_config* cfg, gs_ctx** out) {
     if (cfg->nvrt < 2 || cfg->nvrt > kMaxLevels || cfg->ntr < 0 || cfg->ntr > kMaxTracers || cfg->nz < 1 ||
         cfg->nz > cfg->nvrt)
         return GS_ERR_ARG;
-    if ((cfg->itr_met != 0 && cfg->itr_met != 1 && cfg->itr_met != 3) || cfg->tvd_limiter < 0 ||
+    if ((cfg->itr_met != 0 && cfg->itr_met != 1 && cfg->itr_met != 3 && cfg->itr_met != 4) || cfg->tvd_limiter < 0 ||
         cfg->tvd_limiter > 4 || !(cfg->dfh0 >= 0.0))
         return GS_ERR_ARG;
     gs_ctx* c = new gs_ctx();
@@ -572,7 +572,9 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     if (e == cudaSuccess) { e = dalloc(c, d.egeo, NE); if (e == cudaSuccess) e = cudaMemcpyAsync(d.egeo, pr->egeo.data(), pr->egeo.size() * sizeof(ElemGeo), cudaMemcpyHostToDevice, c->own_st); }
     AL(ez, (size_t)nvrt * NE); AL(ew, (size_t)nvrt * NE); AL(Qv, (size_t)nvrt * NE);
     UP(etr, B.etr); AL(prev, (size_t)ntr * nvrt * NE);
-    if (c->cfg.itr_met == 3) AL(tvds, (size_t)ntr * nvrt * NE); AL(maxDt, NE); AL(ghat, NE);
+    if (c->cfg.itr_met >= 3) AL(tvds, (size_t)ntr * nvrt * NE);
+    if (c->cfg.itr_met == 4) AL(vgam, (size_t)nvrt * NE);
+    AL(maxDt, NE); AL(ghat, NE);
     if (ntr >= 2) { AL(rho_n, (size_t)nvrt * NP); AL(rho_e, (size_t)nvrt * NE); }
     UP(mem_np0, B.mem_np0); UP(mem_ne0, B.mem_ne0); UP(elem_member, B.elem_member);
     c->h_vort.assign((size_t)kVortexParams * c->mem.size(), 0.0);
@@ -598,7 +600,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     P.dt = g.dt; P.thetai = g.thetai; P.h0 = g.h0; P.dtb_min = g.dtb_min; P.dtb_max = g.dtb_max;
     P.velmin = g.velmin_btrack; P.rmaxvel = g.rmaxvel; P.dfv0 = g.dfv0; P.coricoef = g.coricoef;
     P.rho0 = g.rho0; P.grav = g.grav; P.dramp = g.dramp; P.ihhat = g.ihhat;
-    P.tvd = (g.itr_met == 3); P.tvd_limiter = g.tvd_limiter; P.dfh0 = g.dfh0;
+    P.tvd = (g.itr_met >= 3); P.tvd_vert = (g.itr_met == 4); P.tvd_limiter = g.tvd_limiter; P.dfh0 = g.dfh0;
     VG& vg = c->vg;
     std::memset(&vg, 0, sizeof(vg));
     vg.nvrt = nvrt; vg.nz = g.nz; vg.h_s = g.h_s; vg.h_c = g.h_c; vg.h0 = g.h0;

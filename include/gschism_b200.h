@@ -74,8 +74,10 @@ typedef struct {
     int device;                            /* CUDA device ordinal */
     int itr_met;                           /* tracer transport: 1 (or 0) first-order upwind, the
                                               reference's scheme; 3 TVD (flux-limited horizontal
-                                              advection, Casulli & Zanolli 2005) */
-    int tvd_limiter;                       /* itr_met = 3: 0 none (first order), 1 minmod,
+                                              advection, Casulli & Zanolli 2005); 4 the TVD of 3
+                                              with a flux-corrected vertical step (Zalesak FCT
+                                              over the implicit upwind solve) */
+    int tvd_limiter;                       /* itr_met = 3, 4: 0 none (first order), 1 minmod,
                                               2 Osher (beta = 2), 3 van Leer, 4 superbee */
     double dfh0;                           /* constant vertical tracer diffusivity (m^2/s), implicit;
                                               0 = none (the reference has none) */
@@ -198,7 +200,8 @@ gs_status gs_set_vortex(gs_ctx* ctx, int member, const gs_vortex* vortex);
 
 /* Device memory a context holding members of these sizes allocates (bytes, an upper bound used
    for admission by HBM footprint).  np/ne/ns/nnz are the sums over the members.  A TVD context
-   (itr_met = 3) allocates ne * nvrt * ntr * 8 bytes more. */
+   (itr_met = 3) allocates ne * nvrt * ntr * 8 bytes more, one with the vertical FCT (itr_met = 4)
+   ne * nvrt * (ntr + 1) * 8 bytes more. */
 size_t gs_footprint_bytes(int nvrt, int ntr, int nmem, int64_t np, int64_t ne, int64_t ns, int64_t nnz);
 
 typedef struct {

@@ -6,7 +6,8 @@
  * no atmospheric pressure, open boundaries with iettype 0/3 (none / tidal harmonics) and
  * ifltype = 0, first-order upwind transport (itr_met = 1, the reference's scheme) or flux-limited
  * TVD horizontal transport (itr_met = 3, restated from Casulli & Zanolli 2005: the reference has
- * no TVD), optional constant vertical tracer diffusivity.
+ * no TVD), the same with a flux-corrected vertical step (itr_met = 4, Zalesak's FCT over the
+ * implicit upwind solve), optional constant vertical tracer diffusivity.
  */
 #ifndef GS_ORACLE_STEP_H
 #define GS_ORACLE_STEP_H
@@ -35,7 +36,7 @@ typedef struct {
     const double* sigma;         /* [nvrt-nz+1] */
     double dt, thetai, h0, dtb_min, dtb_max, velmin_btrack, rmaxvel, dfv0, coricoef, rho0, grav, dramp;
     int ihhat;
-    int itr_met, tvd_limiter;    /* transport: 1 upwind, 3 TVD; limiter 0 none .. 4 superbee */
+    int itr_met, tvd_limiter;    /* transport: 1 upwind, 3 TVD, 4 TVD + vertical FCT; limiter 0 .. 4 */
     double dfh0;                 /* constant vertical tracer diffusivity (implicit) */
 } og_input;
 
@@ -87,6 +88,11 @@ int  og_step(og_model* m, int it);
 void og_counters(const og_model* m, int64_t* out4);
 /* tracer mass sum_e sum_k V_ek C_ek per tracer, with a compensated (two-sum) accumulator */
 void og_tracer_mass(const og_model* m, double* out_ntr);
+/* the flux-corrected vertical step of itr_met = 4 on one column of n prisms (0 at the bottom):
+ * q[j] the flux between prisms j and j+1, v the volumes, co the field before the step, cl the
+ * implicit upwind result; out the corrected field (may be cl).  Returns 0, or -1 for n < 1. */
+int og_fct_column(int n, double dt, const double* q, const double* v, const double* co, const double* cl,
+                  double* out);
 /* initialise: geometry, CSR pattern, cold-start levels (schism_init.py:78-103) */
 int og_model_init(og_model* m);
 

@@ -66,6 +66,20 @@ def declare(L) -> None:
     L.og_tracer_mass.argtypes = [c_void_p, PD]
     L.og_set_solver.argtypes = [c_void_p, c_double, c_int, c_int]
     L.og_set_vortex.argtypes = [c_void_p, PD]
+    L.og_fct_column.argtypes = [c_int, c_double, PD, PD, PD, PD, PD]
+    L.og_fct_column.restype = c_int
+
+
+def fct_column(dt, q, v, co, cl) -> np.ndarray:
+    """The oracle's flux-corrected vertical step of one column (og_fct_column)."""
+    L = _o.lib()
+    n = len(cl)
+    q = np.ascontiguousarray(np.r_[np.asarray(q, float), 0.0][:max(n - 1, 1)])
+    v, co, cl = (np.ascontiguousarray(a, dtype=float) for a in (v, co, cl))
+    out = np.empty(n)
+    if L.og_fct_column(n, float(dt), _pd(q), _pd(v), _pd(co), _pd(cl), _pd(out)) != 0:
+        raise ValueError("og_fct_column: empty column")
+    return out
 
 
 def _pd(a):

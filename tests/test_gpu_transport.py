@@ -1,6 +1,7 @@
 """Transport options on the GPU against the CPU oracle (gpu): the tracer mass budget, the TVD
-horizontal transport with every limiter, implicit vertical diffusion, and the transport stress
-case (closed basin, 40 levels, 5 tracers with sharp fronts, TVD + vertical diffusion)."""
+horizontal transport with every limiter, the flux-corrected vertical step, implicit vertical
+diffusion, and the transport stress case (closed basin, 40 levels, 5 tracers with sharp fronts,
+TVD + vertical diffusion or vertical FCT)."""
 import dataclasses
 
 import numpy as np
@@ -65,6 +66,56 @@ def test_tvd_transport_phase_matches_oracle(native, oracle_lib, limiter):
     assert relerr(g.get(0, "NODE_TR"), o.get("NODE_TR")) <= 1e-12
 
 
+def _fct_case():
+    c = _with(cases.channel(), itr_met=4, tvd_limiter=3, dfh0=1e-3)
+    c.params.dramp = 0.0                      # full tide from the first step: vertical flow by step 5
+    return c
+
+
+def _oracle_substeps(scale):
+    from oracle.step_api import OracleModel
+    c = _fct_case()
+    o = OracleModel(c)
+    o.run(4)
+    dt = c.params.dt
+    o.begin_step(5); o.btrack(); o.prepare_elevation(5 * dt); o.assemble(5 * dt); o.essential_bc()
+    o.jcg_solve(c.params.rtol, c.params.maxiter, c.params.check_every); o.update_elevation()
+    o.momentum(5 * dt); o.vertical_velocity()
+    o.put("SIDE_U2", scale * o.get("SIDE_U2"))
+    o.transport(dt)
+    return o.counters()[1]
+
+
+@pytest.mark.parametrize("parity", ["odd", "even"])
+def test_vertical_fct_phase_matches_oracle(native, oracle_lib, parity):
+    """itr_met = 4 (TVD horizontal passes + flux-corrected vertical step) on the GPU against the
+    oracle from the same state.  The horizontal result sits in prev after an odd number of
+    sub-steps and in etr (so the vertical step runs in place) after an even one; the side fluxes
+    are scaled by a power of two (exact on both sides: the oracle forms them from the side
+    velocities inside its transport, the GPU in its momentum phase) until the sub-step count has
+    the wanted parity."""
+    from gschism_b200.model import Model
+    from oracle.step_api import OracleModel
+    want = 1 if parity == "odd" else 0
+    scale = next(f for f in (1.0, 2.0, 4.0, 8.0, 16.0, 32.0) if _oracle_substeps(f) % 2 == want)
+    c = _fct_case()
+    o = OracleModel(c)
+    o.run(4)
+    g = Model([c])
+    copy_state(o, g)
+    _phases_to_transport(o, g, c, 5)
+    o.put("SIDE_U2", scale * o.get("SIDE_U2"))
+    qh = g.get(0, "SIDE_QH")
+    g.put(0, "SIDE_QH", np.where(qh > -1e30, scale * qh, qh))
+    o.transport(c.params.dt)
+    g.phase("TRANSPORT", 5)
+    assert g.stats(0)["transport_substeps"] == o.counters()[1]
+    assert o.counters()[1] % 2 == want
+    assert g.stats(0)["error_flags"] == 0
+    assert relerr(g.get(0, "ELEM_TR"), o.get("ELEM_TR")) <= 1e-12
+    assert relerr(g.get(0, "NODE_TR"), o.get("NODE_TR")) <= 1e-12
+
+
 def test_tvd_without_limiter_is_upwind_on_gpu(native):
     from gschism_b200.model import Model
     up = Model([cases.channel()])
@@ -75,15 +126,16 @@ def test_tvd_without_limiter_is_upwind_on_gpu(native):
     assert np.array_equal(up.get(0, "NODE_TR"), tv.get(0, "NODE_TR"))
 
 
-@pytest.mark.parametrize("n", [60, 200])
-def test_transport_stress_matches_oracle(native, oracle_lib, n):
+@pytest.mark.parametrize("n,itr_met", [(60, 3), (200, 3), (200, 4)])
+def test_transport_stress_matches_oracle(native, oracle_lib, n, itr_met):
     """Closed basin, 40 levels, 5 tracers with fronts and blobs, wind-driven, TVD (van Leer) with
-    vertical diffusion: GPU vs oracle over 10 steps, tracer bounds and the mass budget; n x n nodes
-    (200 x 200: 40,000 nodes, 1.6M prisms per tracer), the transport-stress configuration's layout
-    at a size the oracle steps in seconds."""
+    vertical diffusion (itr_met = 3) or TVD with the flux-corrected vertical step (itr_met = 4):
+    GPU vs oracle over 10 steps, tracer bounds and the mass budget; n x n nodes (200 x 200: 40,000
+    nodes, 1.6M prisms per tracer), the transport-stress configuration's layout at a size the
+    oracle steps in seconds."""
     from gschism_b200.model import Model
     from oracle.step_api import OracleModel
-    c = cases.transport_stress(n=n, nsteps=10)
+    c = _with(cases.transport_stress(n=n, nsteps=10), itr_met=itr_met)
     o = OracleModel(c)
     g = Model([c])
     tr0 = o.get("ELEM_TR")
