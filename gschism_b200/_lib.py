@@ -30,7 +30,9 @@ EXPORTS = ["gs_grid_build", "gs_ctx_create", "gs_member_add", "gs_ctx_prepare", 
            "gs_get_stats", "gs_tracer_mass", "gs_set_launch", "gs_get_launch", "gs_member_sizes", "gs_jcg_create", "gs_jcg_buffers", "gs_jcg_solve_csr",
            "gs_jcg_check", "gs_jcg_destroy", "gs_jcg_last_error", "gs_jcg_solve_csr_noalloc",
            "gs_set_vortex", "gs_footprint_bytes", "gs_set_wait_limit", "gs_test_stall_solve", "gs_state_get_async",
-           "gs_output_mark", "gs_output_wait", "gs_host_alloc", "gs_host_free"]
+           "gs_output_mark", "gs_output_wait", "gs_host_alloc", "gs_host_free", "gs_set_member_start", "gs_get_step"]
+
+GS_MEMBER_PARKED = 2000000000
 
 
 class GsConfig(ctypes.Structure):
@@ -113,6 +115,8 @@ def load(build_if_missing: bool = False):
                                            c_void_p, ctypes.POINTER(c_int)]
     L.gs_set_vortex.argtypes = [c_void_p, I, ctypes.POINTER(GsVortex)]
     L.gs_set_wait_limit.argtypes = [c_void_p, ctypes.c_longlong]
+    L.gs_set_member_start.argtypes = [c_void_p, I, I]
+    L.gs_get_step.argtypes = [c_void_p, ctypes.POINTER(c_int)]
     L.gs_test_stall_solve.argtypes = [c_void_p, I]
     L.gs_state_get_async.argtypes = [c_void_p, I, I, c_void_p, c_size_t]
     L.gs_output_mark.argtypes = [c_void_p, ctypes.POINTER(ctypes.c_uint64)]

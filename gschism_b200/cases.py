@@ -394,13 +394,22 @@ def storm(seed: int, nmin: int = 10_000, nmax: int = 2_000_000, nvrt: int = 20, 
     c = basin(seed=int(rng.integers(1, 2**31 - 1)), n=side, nvrt=nvrt, nz=max(2, nvrt // 3), ntr=1,
               length=length, amp=amp, shuffle=shuffle, dt=dt)
     c.name = f"storm{seed}"
+    return c, _vortex(rng, length), int(round(hours * 3600.0 / dt))
+
+
+def _vortex(rng, length: float) -> dict:
     heading = rng.uniform(0.0, 2.0 * math.pi)
     # start 3/4 of the domain size behind the centre, so the track crosses the domain
     cx, cy = 0.5 * length, 0.5 * length
-    vortex = dict(x0=cx - 0.75 * length * math.cos(heading), y0=cy - 0.75 * length * math.sin(heading),
-                  heading=heading, speed=rng.uniform(3.0, 8.0), vmax=rng.uniform(20.0, 60.0),
-                  rmax=rng.uniform(20e3, 60e3), holland_b=rng.uniform(1.2, 1.8), rho_air=1.15)
-    return c, vortex, int(round(hours * 3600.0 / dt))
+    return dict(x0=cx - 0.75 * length * math.cos(heading), y0=cy - 0.75 * length * math.sin(heading),
+                heading=heading, speed=rng.uniform(3.0, 8.0), vmax=rng.uniform(20.0, 60.0),
+                rmax=rng.uniform(20e3, 60e3), holland_b=rng.uniform(1.2, 1.8), rho_air=1.15)
+
+
+def storm_on(case: Case, seed: int) -> dict:
+    """A seeded storm (the vortex of `storm`) on an existing square storm mesh: a forecast request
+    for a region whose mesh is already set up."""
+    return _vortex(np.random.default_rng(seed), float(case.x.max() - case.x.min()))
 
 
 # ----------------------------------------------------------------------------------------------

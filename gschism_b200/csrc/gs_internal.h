@@ -139,6 +139,7 @@ struct Dev {
     double *rho_n, *rho_e;         // [nvrt][NP], [nvrt][NE] densities (allocated with >= 2 tracers)
     // members
     int32_t *mem_np0, *mem_ne0;    // entity offsets [nmem+1]
+    double *mem_start;             // [nmem] start step of each member (its step = clk[0] - start)
     double *vort;                  // [nmem][kVortexParams] storm parameters (gs_vortex + enabled flag)
     int32_t *elem_member;          // [NE]
     double *mem_rem, *mem_dtb;     // transport sub-cycling per member

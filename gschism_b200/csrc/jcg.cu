@@ -295,6 +295,12 @@ __device__ void publish_beta(const JcgView& J, int m, int nit, double* sh) {
     publish64(J, m, 2 * nit + 1, 1, (tot[2] == 0.0) ? 0.0 : tot[1] / tot[2]);
 }
 
+// rows of the FP64 loop (p update and q = A p) unrolled per thread
+#ifndef GS_JCG64_ROW_UNROLL
+#define GS_JCG64_ROW_UNROLL 1
+#endif
+constexpr int kRowUnroll64 = GS_JCG64_ROW_UNROLL;
+
 template <bool SELL>
 __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
     __shared__ double sh[4 * 32];
@@ -369,6 +375,7 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
                 any = true;
                 const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
                 double v[1] = {0.0};
+#pragma unroll kRowUnroll64
                 for (int i = r0 + tid; i < r1; i += kThreads) {
                     const double s = row_dot<SELL, double>(J, J.A, i, [&](int c) { return J.z[c] + beta * pc[c]; });
                     const double pi = J.z[i] + beta * pc[i];
@@ -445,6 +452,12 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
 // each, so a neighbour's three values arrive in one 16-byte load and a row's own four in one),
 // then d.
 static_assert(kIrVectors == 9, "ir32 layout");
+
+// rows of the FP32 inner loop unrolled per thread
+#ifndef GS_JCG_IR_ROW_UNROLL
+#define GS_JCG_IR_ROW_UNROLL 1
+#endif
+constexpr int kRowUnroll = GS_JCG_IR_ROW_UNROLL;
 
 // resident blocks per SM the refinement solve is compiled for (register budget)
 #ifndef GS_JCG_IR_MIN_BLOCKS
@@ -702,6 +715,7 @@ __global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgVi
                 any = true;
                 const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
                 double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll kRowUnroll
                 for (int i = r0 + tid; i < r1; i += kThreads) {
                     // a row's (u, w~, s~, p) travel together: one 16-byte load and store per row
                     const float4 o = uwc[i];

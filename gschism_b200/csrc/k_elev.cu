@@ -21,11 +21,35 @@ __device__ __forceinline__ void clock_at(Dev& d, const Phys& P, int it) {
 __global__ void k_clock_set(Dev d, Phys P, int it) { clock_at(d, P, it); }
 __global__ void k_clock_advance(Dev d, Phys P) { clock_at(d, P, (int)d.clk[0] + 1); }
 
-__global__ void k_elev_bc(Dev d) {
+// Member of node i (mem_np0[m] <= i < mem_np0[m + 1]).
+__device__ __forceinline__ int member_of_node(const Dev& d, int i) {
+    int lo = 0, hi = d.nmem;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (d.mem_np0[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// A member's own clock: its step is the context's step minus the member's start step
+// (gs_set_member_start; 0 unless the member was admitted later), with the time and ramp of that
+// step, so a member admitted into a running context sees the clock of a run of its own.  A
+// member whose start lies ahead of the context's step is parked: time 0, ramp 0 (no tide, no
+// storm).
+__device__ __forceinline__ void member_clock(const Dev& d, const Phys& P, int m, double& time, double& ramp) {
+    const double ls = d.clk[0] - d.mem_start[m];
+    if (ls < 0.0) { time = 0.0; ramp = 0.0; return; }
+    const int it = (int)ls;
+    time = it * P.dt;
+    ramp = (P.dramp > 0.0) ? tanh(2.0 * time / 86400.0 / P.dramp) : 1.0;
+}
+
+__global__ void k_elev_bc(Dev d, Phys P) {
     // computeElevationBoundaryConditions, mdc:4276-4339 (iettype 3: tidal harmonics)
-    const double time = d.clk[1], ramp = d.clk[2];
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < d.NB; b += gridDim.x * blockDim.x) {
         const int i = d.bn_node[b];
+        double time, ramp;
+        member_clock(d, P, member_of_node(d, i), time, ramp);
         const int iettype = d.bn_ietype[b];
         const double eic = 0.0;
         const double r_eic = (1.0 - ramp) * eic;
@@ -253,16 +277,14 @@ __global__ void k_update_elev(Dev d, VG vg) {
 
 // Storm forcing: kinematic surface stress of a radial vortex on a straight track (gs_vortex in the
 // C ABI) for the nodes of members that have one; other members keep their stress.
-__global__ void k_vortex_tau(Dev d, double rho0) {
-    const double time = d.clk[1], ramp = d.clk[2];
+__global__ void k_vortex_tau(Dev d, Phys P) {
+    const double rho0 = P.rho0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.NP; i += gridDim.x * blockDim.x) {
-        int lo = 0, hi = d.nmem;                       // member of node i: mem_np0[lo] <= i < mem_np0[lo+1]
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (d.mem_np0[mid] <= i) lo = mid; else hi = mid;
-        }
+        const int lo = member_of_node(d, i);
         const double* v = d.vort + (size_t)kVortexParams * lo;
         if (v[8] == 0.0) continue;
+        double time, ramp;
+        member_clock(d, P, lo, time, ramp);
         const double x0 = v[0], y0 = v[1], hd = v[2], sp = v[3], vmax = v[4], rmax = v[5], B = v[6], rho_air = v[7];
         const double ch = cos(hd), sh = sin(hd);
         const double cx = x0 + sp * time * ch, cy = y0 + sp * time * sh;
@@ -289,8 +311,8 @@ void launch_clock_set(const Dev& d, const Phys& P, int it, cudaStream_t st) { k_
 void launch_clock_advance(const Dev& d, const Phys& P, cudaStream_t st) { k_clock_advance<<<1, 1, 0, st>>>(d, P); }
 
 void launch_elev_prepare(const Dev& d, const Phys& P, bool vortex, cudaStream_t st, int nsm, const LaunchTable& L) {
-    if (vortex) k_vortex_tau<<<grid_for(d.NP, 256, nsm * 8), 256, 0, st>>>(d, P.rho0);
-    if (d.NB > 0) k_elev_bc<<<grid_for(d.NB, 128, nsm * 4), 128, 0, st>>>(d);
+    if (vortex) k_vortex_tau<<<grid_for(d.NP, 256, nsm * 8), 256, 0, st>>>(d, P);
+    if (d.NB > 0) k_elev_bc<<<grid_for(d.NB, 128, nsm * 4), 128, 0, st>>>(d, P);
     const LaunchShape &sp = L.k[LK_SIDE_PREP], &gh = L.k[LK_GHAT];
     k_side_prep<<<grid_of(d.NS, sp, nsm), sp.block, 0, st>>>(d, P);
     k_ghat<<<grid_of(d.NE, gh, nsm), gh.block, 0, st>>>(d, P);

@@ -579,6 +579,7 @@ extern "C" gs_status gs_ctx_finalize(gs_ctx* c) {
     UP(mem_np0, B.mem_np0); UP(mem_ne0, B.mem_ne0); UP(elem_member, B.elem_member);
     c->h_vort.assign((size_t)kVortexParams * c->mem.size(), 0.0);
     UP(vort, c->h_vort);
+    AL(mem_start, d.nmem);
     AL(mem_rem, 2 * (size_t)d.nmem); AL(mem_dtb, d.nmem); AL(mem_mindt, 2 * (size_t)d.nmem + 1); AL(mem_nsub, d.nmem);
     AL(clk, 3); AL(bar, 1); AL(err, 1); AL(counters, 4);
     d.wait_polls = kWaitPolls;
@@ -1217,6 +1218,25 @@ extern "C" gs_status gs_set_vortex(gs_ctx* c, int member, const gs_vortex* v) {
     return GS_OK;
 }
 
+extern "C" gs_status gs_set_member_start(gs_ctx* c, int member, int start_step) {
+    if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size() || start_step < 0) return GS_ERR_ARG;
+    const double t0 = (double)start_step;
+    cudaError_t e = cudaMemcpyAsync(c->d.mem_start + member, &t0, sizeof(double), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    return GS_OK;
+}
+
+extern "C" gs_status gs_get_step(gs_ctx* c, int* step) {
+    if (!c || !c->finalized || !step) return GS_ERR_ARG;
+    double clk = 0.0;
+    cudaError_t e = cudaMemcpyAsync(&clk, c->d.clk, sizeof(double), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) return c->fail(GS_ERR_CUDA, cudaGetErrorString(e));
+    *step = (int)clk;
+    return GS_OK;
+}
+
 // Upper bound of the device bytes gs_ctx_finalize allocates for members of these total sizes
 // (the allocation list of gs_ctx_finalize and jcg_work_alloc; boundary nodes counted as all nodes,
 // SELL padding as a quarter of the entries, plus allocation granularity).
@@ -1231,7 +1251,7 @@ extern "C" size_t gs_footprint_bytes(int nvrt, int ntr, int nmem, int64_t np, in
     b += (double)ns * (16.0 + 70.0 + 72.0 + 16.0 + 48.0 + L * 52.0 + 4.0);
     b += std::max(L * 16.0 * (double)ns, L * 8.0 * T * (double)ne);   // field exchange staging (largest field)
     b += sell * 16.0 + (double)np / 32.0 * 8.0;
-    b += ((double)np / 1024.0 + nmem) * 84.0 + (double)nmem * (16.0 + 72.0 + 40.0 + 8.0 * kVortexParams + 64.0);
+    b += ((double)np / 1024.0 + nmem) * 84.0 + (double)nmem * (16.0 + 72.0 + 40.0 + 8.0 * kVortexParams + 64.0 + 8.0);
     b += (double)kMassBlocks * kMaxTracers * 16.0 + kMaxTracers * 8.0;
     b += 256.0 * 1024 * 1024;                   // allocation granularity of ~120 allocations
     return (size_t)b;

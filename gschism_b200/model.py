@@ -12,7 +12,7 @@ launches over the batch.
 from __future__ import annotations
 
 import ctypes
-from typing import List, Sequence
+from typing import Dict, List, Sequence
 
 import numpy as np
 
@@ -25,8 +25,21 @@ FIELDS = dict(ETA1=0, ETA2=1, NODE_Z=2, NODE_U2=3, NODE_W2=4, NODE_TR=5, NODE_KB
               ELEM_Z=30, ELEM_W=31, ELEM_QV=32, ELEM_TR=33, ELEM_KB=34, ELEM_DRY=35, ELEM_GHAT=36,
               CSR_DATA=40, CSR_INDPTR=41, CSR_INDICES=42, JCG_X=43, ELBC=44, JCG_X1=45, JCG_X2=46, NODE_RHO=47,
               ELEM_RHO=48)
+# the fields one step reads from the step before
+STATE_FIELDS = ("ETA1", "ETA2", "NODE_Z", "NODE_U2", "NODE_W2", "NODE_TR", "NODE_KB", "NODE_DRY", "SIDE_U2",
+                "SIDE_ZC", "SIDE_KB", "SIDE_DRY", "ELEM_Z", "ELEM_TR", "ELEM_KB", "ELEM_DRY", "JCG_X", "JCG_X1",
+                "JCG_X2")
 INT_FIELDS = {"NODE_KB", "NODE_DRY", "SIDE_KB", "SIDE_DRY", "SIDE_BTELEM", "ELEM_KB", "ELEM_DRY",
               "CSR_INDPTR", "CSR_INDICES"}
+
+
+def _same_batch(a: Case, b: Case) -> bool:
+    """The context takes the vertical grid and the physics constants from its first member."""
+    va, vb = a.vgrid, b.vgrid
+    same_vg = (va.nvrt == vb.nvrt and va.nz == vb.nz and va.h_s == vb.h_s and va.h_c == vb.h_c
+               and va.theta_b == vb.theta_b and va.theta_f == vb.theta_f
+               and np.array_equal(va.ztot, vb.ztot) and np.array_equal(va.sigma, vb.sigma))
+    return same_vg and a.ntracers == b.ntracers and a.params == b.params
 
 
 def footprint_bytes(cases: Sequence[Case]) -> int:
@@ -69,9 +82,11 @@ class Model:
         c0 = self.cases[0]
         vg, p = c0.vgrid, c0.params
         for c in self.cases[1:]:
-            if c.vgrid.nvrt != vg.nvrt or c.ntracers != c0.ntracers or c.params.dt != p.dt:
-                raise ValueError("members of one batch share nvrt, ntracers and dt")
+            if not _same_batch(c, c0):
+                raise ValueError("members of one batch share the vertical grid, the tracer count and the "
+                                 "physics parameters (Params)")
         self._keep = []
+        self._pinned = []
         k = self._k
         cfg = L.GsConfig()
         cfg.nvrt, cfg.ntr, cfg.nz = vg.nvrt, c0.ntracers, vg.nz
@@ -144,6 +159,9 @@ class Model:
         if getattr(self, "h", None):
             self.lib.gs_ctx_destroy(self.h)
             self.h = None
+        for rec in getattr(self, "_pinned", []):
+            rec.free()
+        self._pinned = []
 
     def __del__(self):
         try:
@@ -240,6 +258,14 @@ class Model:
 
     def get(self, member: int, name: str) -> np.ndarray:
         out = np.zeros(self.shape(member, name), dtype=np.int32 if name in INT_FIELDS else np.float64)
+        return self.get_into(member, name, out)
+
+    def get_into(self, member: int, name: str, out: np.ndarray) -> np.ndarray:
+        """gs_state_get into a caller array of the field's shape and type (page-locked memory
+        takes a direct copy)."""
+        if out.shape != self.shape(member, name) or out.dtype != (np.int32 if name in INT_FIELDS else np.float64) \
+                or not out.flags.c_contiguous:
+            raise ValueError(f"{name}: wrong output array")
         L.check(self.lib.gs_state_get(self.h, member, FIELDS[name], out.ctypes.data_as(ctypes.c_void_p),
                                       out.nbytes), self.h, f"gs_state_get {name}")
         return out
@@ -263,3 +289,51 @@ class Model:
     def set_tau(self, member: int, tau) -> None:
         a = np.ascontiguousarray(tau, dtype=np.float64)
         L.check(self.lib.gs_set_tau(self.h, member, _pd(a)), self.h, "gs_set_tau")
+
+    # ----------------------------------------------------------------------------- slots
+    def member_state(self, member: int, pinned: bool = False) -> Dict[str, np.ndarray]:
+        """The fields a step reads from the step before (every other field is recomputed before
+        use), in reference numbering: taken right after construction it is the member's
+        cold-start state.  `pinned`: in page-locked buffers owned by this Model (freed by close),
+        so that putting the state back is one direct copy per field."""
+        if not pinned:
+            return {f: self.get(member, f) for f in STATE_FIELDS}
+        from .output import _PinnedRecord
+        rec = _PinnedRecord(self.lib, {f: self.shape(member, f) for f in STATE_FIELDS},
+                            {f: (np.int32 if f in INT_FIELDS else np.float64) for f in STATE_FIELDS})
+        self._pinned.append(rec)
+        for f in STATE_FIELDS:
+            self.get_into(member, f, rec.arrays[f])
+        return rec.arrays
+
+    def put_member_state(self, member: int, state: Dict[str, np.ndarray]) -> None:
+        for f in STATE_FIELDS:
+            self.put(member, f, state[f])
+
+    def set_member_start(self, member: int, start: int) -> None:
+        """The member's own step = the context's step - start (gs_set_member_start); a start
+        above the context's step parks it (L.GS_MEMBER_PARKED: for good)."""
+        L.check(self.lib.gs_set_member_start(self.h, int(member), int(start)), self.h, "gs_set_member_start")
+
+    def current_step(self) -> int:
+        s = ctypes.c_int()
+        L.check(self.lib.gs_get_step(self.h, ctypes.byref(s)), self.h, "gs_get_step")
+        return s.value
+
+    def admit(self, member: int, cold: Dict[str, np.ndarray], tau=None, vortex=None) -> int:
+        """Start a new run in a member slot at the next step: its cold-start state, its forcing,
+        and its clock from step 1.  Returns the context step the run started after."""
+        self.put_member_state(member, cold)
+        n = self.shape(member, "NODE_TAU")
+        self.set_tau(member, np.zeros(n) if tau is None else tau)
+        self.set_vortex(member, vortex)
+        start = self.current_step()
+        self.set_member_start(member, start)
+        return start
+
+    def park(self, member: int, cold: Dict[str, np.ndarray]) -> None:
+        """Retire the member's run: back to its cold-start state, no stress, no storm, parked."""
+        self.set_member_start(member, L.GS_MEMBER_PARKED)
+        self.set_vortex(member, None)
+        self.set_tau(member, np.zeros(self.shape(member, "NODE_TAU")))
+        self.put_member_state(member, cold)

@@ -23,6 +23,10 @@ order), so each forecast is the same alone and in the mix.
 
 Reported: time-to-forecast per request (arrival to results on the host), its p50/p99, and the
 node-level-steps/s of the whole run.
+
+Slot serving (`SlotServer`, `--regions R`): for a service over a fixed set of region meshes, one
+context holds member slots on those meshes and a request joins the running launch sequence at
+the next step boundary, with its own clock on the device (gs_set_member_start); see the class.
 """
 from __future__ import annotations
 
@@ -51,6 +55,8 @@ class Request:
     finished: float = math.nan     # results on the host
     cohort: int = -1
     result: Optional[np.ndarray] = None
+    region: int = -1               # slot serving: the index of the request's mesh among the regions
+    slot: int = -1                 # slot serving: the member slot it ran in
 
     @property
     def time_to_forecast(self) -> float:
@@ -266,6 +272,152 @@ class Server:
         return list(requests)
 
 
+class SlotEngine:
+    """GPU engine for slot serving: one batch context whose members are slots on the regions'
+    meshes; each slot keeps its cold-start state in page-locked memory, so an admission puts it
+    back with one direct copy per field."""
+
+    def __init__(self, precision: str = "fp32_ir", device: int = 0, fields: Sequence[str] = ("ETA2",)):
+        import torch
+        self.torch = torch
+        self.precision, self.device, self.fields = precision, device, tuple(fields)
+        torch.cuda.set_device(device)
+        self.stream = torch.cuda.Stream(device)
+        self.cold: List[Dict[str, np.ndarray]] = []
+
+    def build(self, slot_cases):
+        from .model import Model
+        h = Model(list(slot_cases), precision=self.precision, device=self.device)
+        self.cold = [h.member_state(i, pinned=True) for i in range(len(slot_cases))]
+        for i in range(len(slot_cases)):
+            h.park(i, self.cold[i])
+        h.sync()
+        h.set_stream(self.stream.cuda_stream)
+        return h
+
+    def admit(self, h, slot: int, r: Request) -> None:
+        h.admit(slot, self.cold[slot], vortex=r.vortex)
+
+    def advance(self, h, k: int) -> None:
+        h.step(k)
+
+    def wait(self) -> None:
+        self.stream.synchronize()
+
+    def result(self, h, slot: int) -> Dict[str, np.ndarray]:
+        return {f: h.get(slot, f).copy() for f in self.fields}
+
+    def park(self, h, slot: int) -> None:
+        h.park(slot, self.cold[slot])
+
+    def close(self, h) -> None:
+        h.close()
+
+
+class SlotServer:
+    """Slot-level continuous batching.  One context holds member slots on a fixed set of meshes
+    (the regions a forecast service covers, `slots_per_region` slots each); a request names its
+    region, its forcing and its horizon.  At every step boundary the server admits queued
+    requests, in arrival order, into free slots of their region (a request whose region is full
+    waits; requests behind it for other regions go ahead): the slot's cold-start state is put back
+    and its clock starts, so the forecast joins the running launch sequence and steps alongside
+    the forecasts already there, exactly as it would alone.  A turn runs until the next forecast
+    reaches its horizon (at most `steps_per_turn` steps); a finished forecast hands back its
+    results and its slot is parked (at rest, no forcing) until the next admission."""
+
+    def __init__(self, engine, regions: Sequence[Any], slots_per_region: Sequence[int] | int = 2,
+                 steps_per_turn: int = 8, clock: Callable[[], float] = time.perf_counter,
+                 sleep: Callable[[float], None] = time.sleep, on_finish: Optional[Callable[[Request], None]] = None):
+        self.engine, self.regions = engine, list(regions)
+        if isinstance(slots_per_region, int):
+            slots_per_region = [slots_per_region] * len(self.regions)
+        self.slot_region: List[int] = [g for g, n in enumerate(slots_per_region) for _ in range(int(n))]
+        if not self.slot_region:
+            raise ValueError("no slots")
+        self.steps_per_turn = int(steps_per_turn)
+        self.clock, self.sleep, self.on_finish = clock, sleep, on_finish
+        self.log: List[tuple] = []
+        self.setup_s = math.nan
+
+    def run(self, requests: Sequence[Request]) -> List[Request]:
+        for r in requests:
+            if not (0 <= r.region < len(self.regions)) or r.region not in self.slot_region:
+                raise ValueError(f"request {r.rid}: no slot for region {r.region}")
+        pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
+        queue: List[Request] = []
+        ts = self.clock()
+        h = self.engine.build([self.regions[g] for g in self.slot_region])
+        self.setup_s = self.clock() - ts
+        free = {g: [s for s, gg in enumerate(self.slot_region) if gg == g] for g in set(self.slot_region)}
+        running: Dict[int, list] = {}          # slot -> [request, steps left]
+        t0 = self.clock()
+        try:
+            while pending or queue or running:
+                now = self.clock() - t0
+                while pending and pending[0].arrival <= now:
+                    queue.append(pending.pop(0))
+                for r in list(queue):
+                    if free[r.region]:
+                        slot = free[r.region].pop(0)
+                        self.engine.admit(h, slot, r)
+                        r.slot, r.cohort = slot, 0
+                        r.admitted = r.started = self.clock() - t0
+                        running[slot] = [r, int(r.nsteps)]
+                        queue.remove(r)
+                        self.log.append(("admit", r.admitted, r.rid, slot))
+                if not running:
+                    self.sleep(max(0.0, pending[0].arrival - now) if pending else 0.002)
+                    continue
+                k = min(self.steps_per_turn, min(left for _, left in running.values()))
+                tt = self.clock()
+                self.engine.advance(h, k)
+                self.engine.wait()
+                self.log.append(("turn", tt - t0, self.clock() - tt, len(running), k))
+                for slot in sorted(running):
+                    running[slot][1] -= k
+                for slot in [s for s in sorted(running) if running[s][1] == 0]:
+                    r = running.pop(slot)[0]
+                    r.result = self.engine.result(h, slot)
+                    r.finished = self.clock() - t0
+                    self.engine.park(h, slot)
+                    free[self.slot_region[slot]].append(slot)
+                    self.log.append(("finish", r.finished, r.rid, slot))
+                    if self.on_finish is not None:
+                        self.on_finish(r)
+        finally:
+            self.engine.close(h)
+        return list(requests)
+
+
+def slot_requests(n: int, rate: float, seed: int, regions: Sequence[Any], hours: float = 48.0,
+                  dt: float = 150.0) -> List[Request]:
+    """n storm-surge requests over the regions' meshes: Poisson arrivals (mean gap 1/rate), a
+    uniformly drawn region and a seeded storm on its mesh (cases.storm_on)."""
+    from . import cases
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    nsteps = int(round(hours * 3600.0 / dt))
+    for i in range(n):
+        if i > 0:
+            t += rng.exponential(1.0 / rate)
+        g = int(rng.integers(0, len(regions)))
+        v = cases.storm_on(regions[g], int(rng.integers(1, 2**31 - 1)))
+        out.append(Request(rid=i, case=regions[g], nsteps=nsteps, vortex=v, arrival=t, region=g))
+    return out
+
+
+def region_meshes(nregions: int, nmin: int, nmax: int, seed: int, nvrt: int = 20, dt: float = 150.0) -> List[Any]:
+    """The regions' storm meshes, node counts log-spaced over [nmin, nmax]."""
+    from . import cases
+    out = []
+    for g in range(nregions):
+        target = nmin * (nmax / nmin) ** (g / max(1, nregions - 1))
+        c, _, _ = cases.storm(seed * 1000 + g, nmin=int(target), nmax=int(target) + 1, nvrt=nvrt, dt=dt)
+        out.append(c)
+    return out
+
+
 def summary(reqs: Sequence[Request], makespan: float) -> dict:
     ttf = np.array([r.time_to_forecast for r in reqs])
     nls = sum(r.node_level_steps() for r in reqs)
@@ -307,7 +459,13 @@ def main(argv=None) -> int:
     ap.add_argument("--budget-gb", type=float, default=None)
     ap.add_argument("--steps-per-turn", type=int, default=8)
     ap.add_argument("--precision", choices=["fp64", "fp32_ir"], default="fp32_ir")
+    ap.add_argument("--regions", type=int, default=0,
+                    help="slot serving over this many region meshes (node counts log-spaced over "
+                         "[nmin, nmax]); 0 = one mesh per request, served in cohorts")
+    ap.add_argument("--slots-per-region", type=int, default=2)
     a = ap.parse_args(argv)
+    if a.regions > 0:
+        return _main_slots(a)
     reqs = poisson_requests(a.requests, a.rate, a.seed, hours=a.hours, nmin=a.nmin, nmax=a.nmax)
     eng = ModelEngine(precision=a.precision)
 
@@ -324,6 +482,28 @@ def main(argv=None) -> int:
     out = summary(reqs, time.perf_counter() - t0)
     out.update({"horizon_hours": a.hours, "rate_per_s": a.rate, "nodes": [int(r.case.n_nodes) for r in reqs],
                 "ttf_s": [round(r.time_to_forecast, 3) for r in reqs], "peak_budget_gb": srv.peak_used / 1e9})
+    print(json.dumps(out))
+    return 0
+
+
+def _main_slots(a) -> int:
+    regions = region_meshes(a.regions, a.nmin, a.nmax, a.seed)
+    reqs = slot_requests(a.requests, a.rate, a.seed, regions, hours=a.hours)
+
+    def progress(r: Request) -> None:
+        print(json.dumps({"rid": r.rid, "region": r.region, "slot": r.slot, "nodes": int(r.case.n_nodes),
+                          "arrival_s": round(r.arrival, 3), "admitted_s": round(r.admitted, 3),
+                          "ttf_s": round(r.time_to_forecast, 3)}), file=sys.stderr, flush=True)
+
+    srv = SlotServer(SlotEngine(precision=a.precision), regions, a.slots_per_region, steps_per_turn=a.steps_per_turn,
+                     on_finish=progress)
+    t0 = time.perf_counter()
+    srv.run(reqs)
+    out = summary(reqs, time.perf_counter() - t0 - srv.setup_s)
+    out.update({"mode": "slots", "horizon_hours": a.hours, "rate_per_s": a.rate,
+                "region_nodes": [int(c.n_nodes) for c in regions], "slots_per_region": a.slots_per_region,
+                "setup_s": round(srv.setup_s, 3), "ttf_s": [round(r.time_to_forecast, 3) for r in reqs],
+                "wait_s": [round(r.admitted - r.arrival, 3) for r in reqs]})
     print(json.dumps(out))
     return 0
 

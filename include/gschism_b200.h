@@ -198,6 +198,19 @@ typedef struct {
 } gs_vortex;
 gs_status gs_set_vortex(gs_ctx* ctx, int member, const gs_vortex* vortex);
 
+/* Slot-level admission.  A member's own step is the context's step minus its start step (default
+   0), and its tide, ramp and storm track follow that step: a member given start K while the
+   context is at step K, with its cold-start state put back (gs_state_put), steps from there on as
+   a context of its own would from its step 1, bit for bit.  A start above the context's step
+   parks the member: no tide, no storm, so a member at rest (cold-start state, zero stress) stays
+   at rest and its solve converges at once.  GS_MEMBER_PARKED parks for good.  Between steps
+   only (the call synchronises the context's stream).  No counterpart in the reference, which
+   runs one forecast per process. */
+#define GS_MEMBER_PARKED 2000000000
+gs_status gs_set_member_start(gs_ctx* ctx, int member, int start_step);
+/* The context's step index (the last BEGIN phase's argument, advanced by every gs_step). */
+gs_status gs_get_step(gs_ctx* ctx, int* step);
+
 /* Device memory a context holding members of these sizes allocates (bytes, an upper bound used
    for admission by HBM footprint).  np/ne/ns/nnz are the sums over the members.  A TVD context
    (itr_met = 3) allocates ne * nvrt * ntr * 8 bytes more, one with the vertical FCT (itr_met = 4)
