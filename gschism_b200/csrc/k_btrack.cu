@@ -225,7 +225,11 @@ __device__ void side_btrack(const Dev& d, const VG& vg, const Phys& P, int s, in
 
 }  // namespace
 
-__global__ void __launch_bounds__(128, 8) k_btrack(Dev d, Phys P, VG vg) {
+// resident blocks per SM the backtracking is compiled for (register budget)
+#ifndef GS_BTRACK_MIN_BLOCKS
+#define GS_BTRACK_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(128, GS_BTRACK_MIN_BLOCKS) k_btrack(Dev d, Phys P, VG vg) {
     const int NS = d.NS, NP = d.NP, NE = d.NE, nvrt = P.nvrt;
     const long long total = (long long)NS * nvrt;
     const int ndelt_max = (int)fmax(1.0, P.dt / P.dtb_min);

@@ -390,20 +390,22 @@ class SlotServer:
 
 
 def slot_requests(n: int, rate: float, seed: int, regions: Sequence[Any], hours: float = 48.0,
-                  dt: float = 150.0) -> List[Request]:
+                  dt: float = 150.0, horizons: Optional[Sequence[float]] = None) -> List[Request]:
     """n storm-surge requests over the regions' meshes: Poisson arrivals (mean gap 1/rate), a
-    uniformly drawn region and a seeded storm on its mesh (cases.storm_on)."""
+    uniformly drawn region, a seeded storm on its mesh (cases.storm_on) and a horizon of `hours`,
+    or one drawn uniformly from `horizons` (hours) when given."""
     from . import cases
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
-    nsteps = int(round(hours * 3600.0 / dt))
     for i in range(n):
         if i > 0:
             t += rng.exponential(1.0 / rate)
         g = int(rng.integers(0, len(regions)))
         v = cases.storm_on(regions[g], int(rng.integers(1, 2**31 - 1)))
-        out.append(Request(rid=i, case=regions[g], nsteps=nsteps, vortex=v, arrival=t, region=g))
+        h = hours if not horizons else float(horizons[int(rng.integers(0, len(horizons)))])
+        out.append(Request(rid=i, case=regions[g], nsteps=int(round(h * 3600.0 / dt)), vortex=v, arrival=t,
+                           region=g))
     return out
 
 
@@ -463,6 +465,10 @@ def main(argv=None) -> int:
                     help="slot serving over this many region meshes (node counts log-spaced over "
                          "[nmin, nmax]); 0 = one mesh per request, served in cohorts")
     ap.add_argument("--slots-per-region", type=int, default=2)
+    ap.add_argument("--region-cohorts", action="store_true",
+                    help="with --regions: serve the same requests in cohorts instead of slots (comparison)")
+    ap.add_argument("--horizons", type=str, default="",
+                    help="slot serving: comma-separated horizons in hours drawn per request (mixed horizons)")
     a = ap.parse_args(argv)
     if a.regions > 0:
         return _main_slots(a)
@@ -488,7 +494,19 @@ def main(argv=None) -> int:
 
 def _main_slots(a) -> int:
     regions = region_meshes(a.regions, a.nmin, a.nmax, a.seed)
-    reqs = slot_requests(a.requests, a.rate, a.seed, regions, hours=a.hours)
+    horizons = [float(x) for x in a.horizons.split(",") if x.strip()]
+    reqs = slot_requests(a.requests, a.rate, a.seed, regions, hours=a.hours, horizons=horizons or None)
+    if a.region_cohorts:
+        srv = Server(ModelEngine(precision=a.precision), steps_per_turn=a.steps_per_turn)
+        t0 = time.perf_counter()
+        srv.run(reqs)
+        out = summary(reqs, time.perf_counter() - t0)
+        out.update({"mode": "cohorts", "horizon_hours": horizons or a.hours, "rate_per_s": a.rate,
+                    "nsteps": [r.nsteps for r in reqs], "region": [r.region for r in reqs],
+                    "region_nodes": [int(c.n_nodes) for c in regions],
+                    "ttf_s": [round(r.time_to_forecast, 3) for r in reqs]})
+        print(json.dumps(out))
+        return 0
 
     def progress(r: Request) -> None:
         print(json.dumps({"rid": r.rid, "region": r.region, "slot": r.slot, "nodes": int(r.case.n_nodes),
@@ -500,7 +518,8 @@ def _main_slots(a) -> int:
     t0 = time.perf_counter()
     srv.run(reqs)
     out = summary(reqs, time.perf_counter() - t0 - srv.setup_s)
-    out.update({"mode": "slots", "horizon_hours": a.hours, "rate_per_s": a.rate,
+    out.update({"mode": "slots", "horizon_hours": horizons or a.hours, "rate_per_s": a.rate,
+                "nsteps": [r.nsteps for r in reqs], "region": [r.region for r in reqs],
                 "region_nodes": [int(c.n_nodes) for c in regions], "slots_per_region": a.slots_per_region,
                 "setup_s": round(srv.setup_s, 3), "ttf_s": [round(r.time_to_forecast, 3) for r in reqs],
                 "wait_s": [round(r.admitted - r.arrival, 3) for r in reqs]})

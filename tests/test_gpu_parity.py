@@ -142,6 +142,28 @@ def test_batch_members_independent_of_the_mix(native):
         alone.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32_ir"])
+def test_basin_with_32bit_matrix_slices(native, oracle_lib, precision):
+    """A 250 x 250 basin (62,500 nodes).  Members are renumbered along a Hilbert curve, whose first
+    and last quadrants share an edge: rows there have columns 31,000 to 62,000 rows away, so the
+    SELL layout mixes slices of 16-bit column offsets with slices of 32-bit columns.  Both
+    precisions against the FP64 oracle over 3 steps."""
+    from gschism_b200.model import Model
+    from oracle.step_api import OracleModel
+    c = cases.basin(seed=5, n=250, nvrt=8, nz=3, ntr=1, length=125e3)
+    o = OracleModel(c)
+    g = Model([c], precision=precision)
+    its_o = o.run(3)
+    g.step(3)
+    if precision == "fp64":
+        assert relerr(g.get(0, "ETA2"), o.get("ETA2")) <= 1e-10
+        assert abs(g.stats(0)["jcg_iters"] - its_o[-1]) <= c.params.check_every
+    else:
+        assert np.abs(g.get(0, "ETA2") - o.get("ETA2")).max() <= 1e-6
+    assert relerr(g.get(0, "ELEM_TR"), o.get("ELEM_TR")) <= 1e-8
+    g.close()
+
+
 def test_mixed_precision_elevation_within_1e6_m(native, oracle_lib):
     """FP32 inner JCG with FP64 refinement: elevation within 1e-6 m of the FP64 oracle."""
     from gschism_b200.model import Model
