@@ -143,11 +143,10 @@ def test_batch_members_independent_of_the_mix(native):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32_ir"])
-def test_basin_with_32bit_matrix_slices(native, oracle_lib, precision):
-    """A 250 x 250 basin (62,500 nodes).  Members are renumbered along a Hilbert curve, whose first
-    and last quadrants share an edge: rows there have columns 31,000 to 62,000 rows away, so the
-    SELL layout mixes slices of 16-bit column offsets with slices of 32-bit columns.  Both
-    precisions against the FP64 oracle over 3 steps."""
+def test_basin_62k_nodes_against_oracle(native, oracle_lib, precision):
+    """A 250 x 250 basin (62,500 nodes, 8 levels): a member of many solver tiles, renumbered along
+    a Hilbert curve whose first and last quadrants share an edge (rows there gather columns
+    31,000-62,000 rows away).  Both precisions against the FP64 oracle over 3 steps."""
     from gschism_b200.model import Model
     from oracle.step_api import OracleModel
     c = cases.basin(seed=5, n=250, nvrt=8, nz=3, ntr=1, length=125e3)
