@@ -9,8 +9,9 @@ JCG rtol 1e-12.  Inputs are seeded synthetic data (no dataset involved).
 
 value    = node-level-steps/s of the timed steps (sum of nodes x levels x steps / device time),
            FP32-inner JCG with FP64 refinement ("fp32_ir"), state resident in HBM.
-e2e      = the same loop through the C ABI with page-locked host buffers: every step uploads the
-           surface stress field from host memory (gs_set_tau) and reads the elevation back
+e2e      = the same steps (a fresh context from the same cold start, the same step indices)
+           through the C ABI with page-locked host buffers: every step uploads the surface stress
+           field from host memory (gs_set_tau), steps (gs_step) and reads the elevation back
            (gs_state_get).
 roofline = the JCG persistent kernel (dominant), algorithmic bytes per launch / launch time.
 The plain FP64 single-instance form is measured on the same GPU and reported under "fp64".
@@ -136,10 +137,11 @@ class Clocks:
         return out
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per inner iteration of k_jcg_ir on
-# the 1M-node basin, from the ncu capture summarised in profiles/k_jcg_ir_basin1M.md (launch
-# bytes / inner iterations of that launch); scaled here by the timed launches' inner iterations.
-JCG_DRAM_BYTES_PER_INNER_ITER = 18.7e6
+# DRAM bytes (reads + writes, dram__bytes.sum) per inner iteration of k_jcg_ir on the 1M-node
+# basin, from one ncu capture of that kernel (the second step's solve of the same 1,000,000-row
+# system with 6 levels: launch bytes / inner iterations of that launch); scaled here by the timed
+# launches' inner iterations.
+JCG_DRAM_BYTES_PER_INNER_ITER = 23.9e6
 
 
 def _jcg_bytes_per_iter(N, nnz, mode):
@@ -210,8 +212,13 @@ def run_ours(a):
         res[mode]["jcg_outer_last"] = st["jcg_outer"]
         if mode == "fp32_ir":
             # end-to-end through the C ABI with page-locked host buffers: upload tau, step, read
-            # eta back
+            # eta back; a fresh context from the same cold start, warmed up and timed over the same
+            # step indices as the device-timed loop above (the flow, and with it the work of a
+            # step, grows while the tide ramps up)
             import ctypes
+            m.close()
+            m = Model([case], precision=mode, device=local)
+            m.set_stream(stream.cuda_stream)
             tau_t = torch.from_numpy(np.ascontiguousarray(case.tau)).pin_memory()
             eta_t = torch.zeros(nodes, dtype=torch.float64).pin_memory()
             tau, eta = tau_t.numpy(), eta_t.numpy()
@@ -221,8 +228,8 @@ def run_ours(a):
                 m.step(1)
                 m.lib.gs_state_get(m.h, 0, 1, eta.ctypes.data_as(ctypes.c_void_p), eta.nbytes)
 
-            # untimed warm-up of this path: its first gs_step captures the step graph
-            for _ in range(max(1, min(a.warmup, 3))):
+            # untimed warm-up of this path (its first gs_step captures the step graph)
+            for _ in range(a.warmup):
                 e2e_step()
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
