@@ -6,6 +6,7 @@ Used to drive profiler captures of one phase on a chosen size: the elevation sol
 the horizontal mesh only, so `--levels` can shrink the device state without changing it.
 
     python -m gschism_b200.run_case --n 1000 --steps 12 --time-phase BTRACK --repeat 20
+    python -m gschism_b200.run_case --case ensemble --members 12 --levels 3 --steps 2
 
 times one phase alone on the state reached after the steps (CUDA events around `--repeat`
 launches after 3 untimed ones).  Only phases that do not modify their own inputs give a
@@ -22,7 +23,8 @@ from .model import Model
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--case", choices=["basin", "channel"], default="basin")
+    ap.add_argument("--case", choices=["basin", "channel", "ensemble"], default="basin")
+    ap.add_argument("--members", type=int, default=64, help="ensemble: the first members of the 64-member set")
     ap.add_argument("--n", type=int, default=1000, help="basin lattice side (n x n nodes)")
     ap.add_argument("--levels", type=int, default=30, help="vertical levels (basin)")
     ap.add_argument("--steps", type=int, default=2)
@@ -33,16 +35,19 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     t0 = time.time()
     if a.case == "basin":
-        c = cases.basin(n=a.n, nvrt=a.levels, nz=max(2, min(10, a.levels // 3)))
+        cs = [cases.basin(n=a.n, nvrt=a.levels, nz=max(2, min(10, a.levels // 3)))]
+    elif a.case == "ensemble":
+        cs = cases.ensemble(n_members=64, nvrt=a.levels)[:a.members]
     else:
-        c = cases.channel()
-    m = Model([c], precision=a.precision, ir_inner_rtol=a.inner_rtol)
-    print(f"case {a.case}: {m.sizes[0]['np']} nodes, {c.vgrid.nvrt} levels, set-up {time.time() - t0:.1f} s",
-          flush=True)
+        cs = [cases.channel()]
+    m = Model(cs, precision=a.precision, ir_inner_rtol=a.inner_rtol)
+    print(f"case {a.case}: {sum(z['np'] for z in m.sizes)} nodes in {len(cs)} member(s), {cs[0].vgrid.nvrt} "
+          f"levels, set-up {time.time() - t0:.1f} s", flush=True)
     for s in range(a.steps):
         m.step(1)
         m.sync()
-        print("step", s, m.stats(), flush=True)
+        its = [m.stats(k)["jcg_iters"] for k in range(len(cs))]
+        print("step", s, m.stats(), "iters per member", min(its), "..", max(its), flush=True)
     if a.time_phase:
         import torch
         st = torch.cuda.Stream()
