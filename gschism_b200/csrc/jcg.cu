@@ -484,12 +484,21 @@ __global__ void __launch_bounds__(kThreads) k_jcg64(JcgView J) {
 // then d.
 static_assert(kIrVectors == 9, "ir32 layout");
 
-// rows of the FP32 inner loop unrolled per thread (two rows' gathers in flight: 13% faster on a
-// 1M-row system than one, bit for bit the same; three and four were not faster there)
+// rows of the FP32 inner loop in flight per thread, bit for bit the same result whatever the
+// count: two for a system whose working set fits in L2 (13% faster than one on a 1M-row system;
+// three and four were not faster there), four beyond it (5% faster than two on the 64-member
+// ensemble's 9M rows, where DRAM latency has to be covered)
 #ifndef GS_JCG_IR_ROW_UNROLL
 #define GS_JCG_IR_ROW_UNROLL 2
 #endif
+#ifndef GS_JCG_IR_ROW_UNROLL_LARGE
+#define GS_JCG_IR_ROW_UNROLL_LARGE 4
+#endif
 constexpr int kRowUnroll = GS_JCG_IR_ROW_UNROLL;
+constexpr int kRowUnrollLarge = GS_JCG_IR_ROW_UNROLL_LARGE;
+// bytes an FP32 inner iteration touches per row (matrix slots, indices, the row's float4 state,
+// d and the diagonal), for the L2 test that picks the row count in flight
+constexpr double kIrBytesPerRow = 100.0;
 
 // resident blocks per SM the refinement solve is compiled for (register budget)
 #ifndef GS_JCG_IR_MIN_BLOCKS
@@ -597,7 +606,7 @@ __device__ __forceinline__ void member_arrive(const JcgView& J, int m, int it, i
     st_release_i32(&J.mgen[m], nit);
 }
 
-template <bool SELL>
+template <bool SELL, int UNR>
 __global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgView J) {
     __shared__ double sh[4 * 32];
     __shared__ double pub[3];
@@ -747,7 +756,7 @@ __global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgVi
                 any = true;
                 const int r0 = J.tile_r0[t], r1 = J.tile_r1[t];
                 double v[3] = {0.0, 0.0, 0.0};
-#pragma unroll kRowUnroll
+#pragma unroll UNR
                 for (int i = r0 + tid; i < r1; i += kThreads) {
                     // a row's (u, w~, s~, p) travel together: one 16-byte load and store per row
                     const float4 o = uwc[i];
@@ -788,8 +797,14 @@ __global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgVi
 
 // ------------------------------------------------------------------------------ host ----
 
+static const void* ir_kernel(bool sell, bool large) {
+    if (sell) return large ? (const void*)k_jcg_ir<true, kRowUnrollLarge> : (const void*)k_jcg_ir<true, kRowUnroll>;
+    return large ? (const void*)k_jcg_ir<false, kRowUnrollLarge> : (const void*)k_jcg_ir<false, kRowUnroll>;
+}
+
 struct JcgWork {
     int n = 0, nmem = 0, ntiles = 0, grid = 0, grid64 = 0, gridir = 0;
+    bool ir_large = false;           // the FP32 inner solve's working set exceeds the L2
     bool sell = false;               // kernels instantiated for the SELL-32 layout
     int32_t *tile_r0 = nullptr, *tile_r1 = nullptr, *tile_mem = nullptr, *mem_t0 = nullptr, *mem_t1 = nullptr;
     int32_t *blk64 = nullptr, *blkir = nullptr;
@@ -860,9 +875,14 @@ cudaError_t jcg_work_alloc(JcgWork*& w, const std::vector<int>& row0, const std:
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const void* f64 = sell ? (const void*)k_jcg64<true> : (const void*)k_jcg64<false>;
-    const void* fir = sell ? (const void*)k_jcg_ir<true> : (const void*)k_jcg_ir<false>;
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
+    long long nrows = 0;
+    for (int r : rows) nrows += r;
+    w->ir_large = (double)nrows * kIrBytesPerRow > (double)l2;
     w->sell = sell;
+    const void* f64 = sell ? (const void*)k_jcg64<true> : (const void*)k_jcg64<false>;
+    const void* fir = ir_kernel(sell, w->ir_large);
     w->grid64 = std::max(1, std::min(T, coop_blocks(f64, nsm, tiling.per_sm)));
     w->gridir = std::max(1, std::min(T, coop_blocks(fir, nsm, tiling.per_sm)));
     std::vector<int32_t> b64, bir;
@@ -945,7 +965,7 @@ cudaError_t jcg_launch(const JcgArgs& a, JcgWork* w, cudaStream_t st, int nsm) {
     cudaMemsetAsync(w->mouter, 0, 4 * (5 * (size_t)w->nmem + 2), st);   // mouter .. mcnt, ndone, status
     void* args[] = {&J};
     if ((a.sell != nullptr) != w->sell) return cudaErrorInvalidValue;
-    const void* fn = ir ? (w->sell ? (const void*)k_jcg_ir<true> : (const void*)k_jcg_ir<false>)
+    const void* fn = ir ? ir_kernel(w->sell, w->ir_large)
                         : (w->sell ? (const void*)k_jcg64<true> : (const void*)k_jcg64<false>);
     const int grid = ir ? w->gridir : w->grid64;
     return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, 0, st);
