@@ -44,14 +44,21 @@ def _same_batch(a: Case, b: Case) -> bool:
 
 def footprint_bytes(cases: Sequence[Case]) -> int:
     """Upper bound of the device memory a context holding these members allocates
-    (gs_footprint_bytes).  Side and matrix counts follow from the triangulation: a simply
-    connected triangulated domain has np + ne - 1 sides and np + 2 ns matrix entries."""
+    (gs_footprint_bytes, plus the TVD and vertical-FCT scratch arrays of itr_met 3 and 4).  Side
+    and matrix counts follow from the triangulation: a simply connected triangulated domain has
+    np + ne - 1 sides and np + 2 ns matrix entries."""
     lib = L.load()
     c0 = cases[0]
     npn = sum(c.n_nodes for c in cases)
     ne = sum(c.n_elems for c in cases)
     ns = sum(c.n_nodes + c.n_elems - 1 for c in cases)
-    return int(lib.gs_footprint_bytes(c0.vgrid.nvrt, c0.ntracers, len(cases), npn, ne, ns, npn + 2 * ns))
+    b = int(lib.gs_footprint_bytes(c0.vgrid.nvrt, c0.ntracers, len(cases), npn, ne, ns, npn + 2 * ns))
+    nvrt, ntr, itr = c0.vgrid.nvrt, c0.ntracers, int(c0.params.itr_met)
+    if itr >= 3:
+        b += ne * nvrt * ntr * 8          # TVD inflow sums
+    if itr == 4:
+        b += ne * nvrt * 8                # vertical sweep scratch
+    return b
 
 
 def _pd(a):

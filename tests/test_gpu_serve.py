@@ -80,6 +80,23 @@ def test_served_forecasts_equal_alone(native):
     assert s["ttf_p99_s"] >= s["ttf_p50_s"] > 0
 
 
+def test_footprint_bounds_a_tvd_fct_context(native):
+    """The bound includes the TVD and vertical-FCT scratch arrays (itr_met = 4)."""
+    import dataclasses
+    import torch
+    from gschism_b200.model import Model, footprint_bytes
+    c = cases.transport_stress(n=150, nsteps=10)
+    c.params = dataclasses.replace(c.params, itr_met=4)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    m = Model([c])
+    m.sync()
+    used = free0 - torch.cuda.mem_get_info()[0]
+    est = footprint_bytes([c])
+    m.close()
+    assert used <= est
+
+
 def test_footprint_bounds_the_allocation(native):
     import torch
     from gschism_b200.model import Model, footprint_bytes
