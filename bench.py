@@ -21,6 +21,9 @@ ensemble = the batched form: 64 members on meshes of uneven size (20k-500k nodes
 error_vs_oracle = the FP64 and FP32+IR forms after 3 steps of the benchmarked mesh against the
            CPU oracle (oracle/, pinned to the reference's own kernels by tests/test_ref_pinned.py)
            after the same 3 steps: elevation max |difference| in m, tracers and velocities relative.
+serving = storm-surge forecast requests served in cohorts (p50/p99 time-to-forecast);
+serving_slots = the same kind of requests over four region meshes, admitted into free member
+           slots of one running context at step boundaries.
 cpu_baseline = the oracle on the benchmarked mesh itself (all host threads), 2 timed steps.
 --impl reference = the same oracle on the benchmarked mesh, 1 warm-up + up to 6 timed steps (a
            bounded sample of the run), plus a single-thread figure on a 200 x 200 sample.
@@ -255,6 +258,7 @@ def run_ours(a):
     # the batched-ensemble comparison is a one-GPU measurement (rank 0 of a one-rank run)
     ens = run_ensemble(a, stream, local) if (ws == 1 and not a.no_ensemble) else None
     srv = run_serving(local) if (ws == 1 and not a.no_serve) else None
+    slots = run_slot_serving(local) if (ws == 1 and not a.no_serve) else None
     r = res["fp32_ir"]
     # roofline of the dominant kernel (JCG): algorithmic bytes / average launch time
     nnz = r["nnz"]
@@ -294,6 +298,8 @@ def run_ours(a):
         line["ensemble_sharded"] = ens_sharded
     if srv is not None:
         line["serving"] = srv
+    if slots is not None:
+        line["serving_slots"] = slots
     if not a.no_cpu:
         cb, ofields, case_full = cpu_sample(a)
         line["cpu_baseline"] = cb
@@ -452,6 +458,28 @@ def run_serving(local, n=8, rate=2.0, hours=6.0, seed=1):
                             f"{hours:g} h horizon at dt=150 s (the full scenario's horizon is 48 h)",
                 "nodes": [int(r.case.n_nodes) for r in reqs], "ttf_s": [round(r.time_to_forecast, 3) for r in reqs],
                 "build_s_total": round(sum(builds), 2)})
+    return out
+
+
+def run_slot_serving(local, n=16, rate=2.0, hours=(3.0, 6.0), seed=1, regions=4, slots=2):
+    """Slot-level serving (gschism_b200/serve.py:SlotServer): one context with `slots` member
+    slots on each of `regions` storm meshes (30k-600k nodes, 20 levels); n requests (a region, a
+    storm, a horizon drawn from `hours`) arriving as a Poisson process of `rate` per second, each
+    admitted into a free slot of its region at a step boundary while the others run.  Horizons
+    are a few hours instead of the scenario's 48 h, to keep this run to about half a minute."""
+    from gschism_b200.serve import SlotEngine, SlotServer, region_meshes, slot_requests, summary
+    regs = region_meshes(regions, 30_000, 600_000, seed)
+    reqs = slot_requests(n, rate, seed, regs, horizons=list(hours))
+    srv = SlotServer(SlotEngine(precision="fp32_ir", device=local), regs, slots)
+    t0 = time.perf_counter()
+    srv.run(reqs)
+    out = summary(reqs, time.perf_counter() - t0 - srv.setup_s)
+    out.update({"workload": f"{n} storm-surge requests over {regions} region meshes "
+                            f"({', '.join(str(int(c.n_nodes)) for c in regs)} nodes, 20 levels), {slots} slots each, "
+                            f"Poisson arrivals {rate}/s, horizons {'/'.join(f'{h:g}' for h in hours)} h at dt=150 s",
+                "setup_s": round(srv.setup_s, 2), "ttf_s": [round(r.time_to_forecast, 3) for r in reqs],
+                "wait_s": [round(r.admitted - r.arrival, 3) for r in reqs]})
+    out.pop("cohorts", None)
     return out
 
 

@@ -144,6 +144,9 @@ __device__ __forceinline__ void member_totals_wide(const JcgView& J, int m, cons
 
 __device__ __forceinline__ int ld_done(const JcgView& J, int m) { return *((volatile int32_t*)&J.mdone[m]); }
 
+// generation word of a finished member (mgen), in both solves
+constexpr int kGenRetired = 0x7fffffff;
+
 // Block-uniform read of a word another block may update in the same phase: thread 0 reads,
 // the block agrees on that value (either value leads every block to the same decision).
 __device__ __forceinline__ int uniform_ld(const int32_t* p, int* shv) {
@@ -227,7 +230,9 @@ __device__ void phase_atol(const JcgView& J, double* sh) {
         if (threadIdx.x == 0) {
             const double atol = J.rtol * sqrt(tot[0]);
             J.mem_atol2[m] = atol * atol;
-            if (atol == 0.0) { J.mdone[m] = 0; __threadfence(); atomicAdd(J.ndone, 1u); }
+            // a zero right-hand side: the member is done before the first iteration, and its
+            // generation word says so to every block that holds its tiles
+            if (atol == 0.0) { J.mdone[m] = 0; J.mgen[m] = kGenRetired; __threadfence(); atomicAdd(J.ndone, 1u); }
         }
     }
 }
@@ -250,7 +255,7 @@ __device__ __forceinline__ unsigned arrivals(const JcgView& J, int m) {
 // kRetired a finished member.  The totals, and so alpha, beta, the iterates and the iteration
 // counts, are those of the grid-barrier form bit for bit.
 
-constexpr int kRetired64 = 0x7fffffff;
+constexpr int kRetired64 = kGenRetired;
 
 __device__ __forceinline__ int ld_acquire_s32(const int32_t* p) {
     int v;
@@ -520,7 +525,7 @@ __device__ __forceinline__ int ld_i32(const int32_t* p) { return *((const volati
 // blocks hold its tiles) sums the member's tile partials in tile order, takes the convergence
 // decision, computes the next (alpha, beta) and publishes them with mgen[m] = next iteration (or
 // kRetired).  Blocks wait only for the members they hold.  Every wait is bounded.
-constexpr int kRetired = 0x7fffffff;
+constexpr int kRetired = kGenRetired;
 
 __device__ __forceinline__ int ld_acquire_i32(const int32_t* p) {
     int v;
@@ -671,7 +676,10 @@ __global__ void __launch_bounds__(kThreads, GS_JCG_IR_MIN_BLOCKS) k_jcg_ir(JcgVi
                 const bool owner = (t == J.mem_t0[m] && tid == 0);
                 if (tot[0] <= J.mem_atol2[m]) {
                     if (owner) {
+                        // retired at the outer test: blocks that hold its tiles beside another
+                        // member's see kRetired at every inner iteration instead of waiting
                         J.mdone[m] = J.minner[m]; J.mouter[m] = outer;
+                        J.mgen[m] = kRetired;
                         __threadfence(); atomicAdd(J.ndone, 1u);
                     }
                     continue;

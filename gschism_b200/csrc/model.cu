@@ -1057,6 +1057,12 @@ extern "C" gs_status gs_state_get(gs_ctx* c, int member, int field, void* host, 
     if (!c || !c->finalized || member < 0 || member >= (int)c->mem.size() || !host) return GS_ERR_ARG;
     FieldInfo fi;
     if (!field_info(c, field, fi)) return c->fail(GS_ERR_STATE, "unknown field");
+    // a bounded wait that ran out in the steps before (their results are incomplete) is
+    // reported here, once, like gs_sync
+    {
+        const gs_status s = check_err(c);
+        if (s != GS_OK) return s;
+    }
     MemberHost& m = c->mem[member];
     if (fi.ent == 'C' || fi.ent == 'R') {
         if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->fail(GS_ERR_CUDA, "sync");

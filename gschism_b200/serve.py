@@ -37,7 +37,7 @@ import json
 import math
 import sys
 import time
-from typing import Any, Callable, Dict, List, Optional, Sequence
+from typing import Any, Callable, Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -273,30 +273,35 @@ class Server:
 
 
 class SlotEngine:
-    """GPU engine for slot serving: one batch context whose members are slots on the regions'
-    meshes; each slot keeps its cold-start state in page-locked memory, so an admission puts it
-    back with one direct copy per field."""
+    """GPU engine for slot serving: one batch context per region, its members the region's slots
+    on the region's mesh; each slot keeps its cold-start state in page-locked memory, so an
+    admission puts it back with one direct copy per field.  All contexts step on one stream."""
 
-    def __init__(self, precision: str = "fp32_ir", device: int = 0, fields: Sequence[str] = ("ETA2",)):
+    def __init__(self, precision: str = "fp32_ir", device: int = 0, fields: Sequence[str] = ("ETA2",),
+                 jcg_tiles: Optional[Tuple[int, int]] = None):
         import torch
         self.torch = torch
         self.precision, self.device, self.fields = precision, device, tuple(fields)
+        self.jcg_tiles = jcg_tiles            # (tiles of a large member, smallest tile), or the default
         torch.cuda.set_device(device)
         self.stream = torch.cuda.Stream(device)
-        self.cold: List[Dict[str, np.ndarray]] = []
+        self.cold: Dict[int, List[Dict[str, np.ndarray]]] = {}
 
     def build(self, slot_cases):
         from .model import Model
         h = Model(list(slot_cases), precision=self.precision, device=self.device)
-        self.cold = [h.member_state(i, pinned=True) for i in range(len(slot_cases))]
+        if self.jcg_tiles is not None:
+            h.set_launch("JCG_TILES", *self.jcg_tiles)
+        cold = [h.member_state(i, pinned=True) for i in range(len(slot_cases))]
         for i in range(len(slot_cases)):
-            h.park(i, self.cold[i])
+            h.park(i, cold[i])
         h.sync()
         h.set_stream(self.stream.cuda_stream)
+        self.cold[id(h)] = cold
         return h
 
     def admit(self, h, slot: int, r: Request) -> None:
-        h.admit(slot, self.cold[slot], vortex=r.vortex)
+        h.admit(slot, self.cold[id(h)][slot], vortex=r.vortex)
 
     def advance(self, h, k: int) -> None:
         h.step(k)
@@ -304,88 +309,127 @@ class SlotEngine:
     def wait(self) -> None:
         self.stream.synchronize()
 
+    def check(self, h) -> None:
+        """Raise if a bounded device wait ran out during the turn (gs_sync)."""
+        h.sync()
+
     def result(self, h, slot: int) -> Dict[str, np.ndarray]:
         return {f: h.get(slot, f).copy() for f in self.fields}
 
     def park(self, h, slot: int) -> None:
-        h.park(slot, self.cold[slot])
+        h.park(slot, self.cold[id(h)][slot])
 
     def close(self, h) -> None:
+        self.cold.pop(id(h), None)
         h.close()
 
 
+@dataclasses.dataclass
+class _Region:
+    g: int                          # region index
+    nodes: int                      # nodes of one slot
+    handle: Any = None              # its context
+    free: List[int] = dataclasses.field(default_factory=list)
+    running: Dict[int, list] = dataclasses.field(default_factory=dict)   # slot -> [request, steps left]
+
+
 class SlotServer:
-    """Slot-level continuous batching.  One context holds member slots on a fixed set of meshes
-    (the regions a forecast service covers, `slots_per_region` slots each); a request names its
-    region, its forcing and its horizon.  At every step boundary the server admits queued
+    """Slot-level continuous batching.  Every region a forecast service covers (one mesh each)
+    gets one context of `slots_per_region` member slots on its mesh, built once; a request names
+    its region, its forcing and its horizon.  At every step boundary the server admits queued
     requests, in arrival order, into free slots of their region (a request whose region is full
     waits; requests behind it for other regions go ahead): the slot's cold-start state is put back
-    and its clock starts, so the forecast joins the running launch sequence and steps alongside
-    the forecasts already there, exactly as it would alone.  A turn runs until the next forecast
-    reaches its horizon (at most `steps_per_turn` steps); a finished forecast hands back its
-    results and its slot is parked (at rest, no forcing) until the next admission."""
+    and its clock starts, so the forecast joins the running launch sequence of its region and
+    steps alongside the forecasts already there, exactly as it would alone.  Each turn advances
+    every region that has forecasts running by about `turn_node_steps` node-steps (a small
+    region's context many steps, a large one's few; at most `steps_per_turn`, and never past the
+    next horizon); regions with nothing running are not stepped.  A finished forecast hands back
+    its results and its slot is parked (at rest, no forcing) until the next admission."""
 
     def __init__(self, engine, regions: Sequence[Any], slots_per_region: Sequence[int] | int = 2,
-                 steps_per_turn: int = 8, clock: Callable[[], float] = time.perf_counter,
+                 steps_per_turn: int = 32, turn_node_steps: Optional[int] = 4_000_000,
+                 clock: Callable[[], float] = time.perf_counter,
                  sleep: Callable[[float], None] = time.sleep, on_finish: Optional[Callable[[Request], None]] = None):
         self.engine, self.regions = engine, list(regions)
         if isinstance(slots_per_region, int):
             slots_per_region = [slots_per_region] * len(self.regions)
-        self.slot_region: List[int] = [g for g, n in enumerate(slots_per_region) for _ in range(int(n))]
-        if not self.slot_region:
+        self.nslots = [int(n) for n in slots_per_region]
+        if not any(self.nslots):
             raise ValueError("no slots")
-        self.steps_per_turn = int(steps_per_turn)
+        self.steps_per_turn, self.turn_node_steps = int(steps_per_turn), turn_node_steps
         self.clock, self.sleep, self.on_finish = clock, sleep, on_finish
         self.log: List[tuple] = []
         self.setup_s = math.nan
 
+    def _turn_steps(self, reg: _Region) -> int:
+        k = self.steps_per_turn
+        if self.turn_node_steps:
+            ctx_nodes = reg.nodes * len(reg.free) + reg.nodes * len(reg.running)
+            k = max(1, min(k, int(self.turn_node_steps // max(1, ctx_nodes))))
+        return min(k, min(left for _, left in reg.running.values()))
+
     def run(self, requests: Sequence[Request]) -> List[Request]:
         for r in requests:
-            if not (0 <= r.region < len(self.regions)) or r.region not in self.slot_region:
+            if not (0 <= r.region < len(self.regions)) or self.nslots[r.region] < 1:
                 raise ValueError(f"request {r.rid}: no slot for region {r.region}")
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
         queue: List[Request] = []
         ts = self.clock()
-        h = self.engine.build([self.regions[g] for g in self.slot_region])
+        regs: List[_Region] = []
+        for g, n in enumerate(self.nslots):
+            if n < 1:
+                continue
+            reg = _Region(g=g, nodes=int(self.regions[g].n_nodes), free=list(range(n)))
+            reg.handle = self.engine.build([self.regions[g]] * n)
+            regs.append(reg)
+        by_g = {reg.g: reg for reg in regs}
         self.setup_s = self.clock() - ts
-        free = {g: [s for s, gg in enumerate(self.slot_region) if gg == g] for g in set(self.slot_region)}
-        running: Dict[int, list] = {}          # slot -> [request, steps left]
         t0 = self.clock()
         try:
-            while pending or queue or running:
+            while pending or queue or any(reg.running for reg in regs):
                 now = self.clock() - t0
                 while pending and pending[0].arrival <= now:
                     queue.append(pending.pop(0))
                 for r in list(queue):
-                    if free[r.region]:
-                        slot = free[r.region].pop(0)
-                        self.engine.admit(h, slot, r)
-                        r.slot, r.cohort = slot, 0
+                    reg = by_g[r.region]
+                    if reg.free:
+                        slot = reg.free.pop(0)
+                        self.engine.admit(reg.handle, slot, r)
+                        r.slot, r.cohort = slot, r.region
                         r.admitted = r.started = self.clock() - t0
-                        running[slot] = [r, int(r.nsteps)]
+                        reg.running[slot] = [r, int(r.nsteps)]
                         queue.remove(r)
-                        self.log.append(("admit", r.admitted, r.rid, slot))
-                if not running:
+                        self.log.append(("admit", r.admitted, r.rid, r.region, slot))
+                active = [reg for reg in regs if reg.running]
+                if not active:
                     self.sleep(max(0.0, pending[0].arrival - now) if pending else 0.002)
                     continue
-                k = min(self.steps_per_turn, min(left for _, left in running.values()))
                 tt = self.clock()
-                self.engine.advance(h, k)
+                ks = []
+                for reg in active:
+                    k = self._turn_steps(reg)
+                    self.engine.advance(reg.handle, k)
+                    ks.append((reg, k))
                 self.engine.wait()
-                self.log.append(("turn", tt - t0, self.clock() - tt, len(running), k))
-                for slot in sorted(running):
-                    running[slot][1] -= k
-                for slot in [s for s in sorted(running) if running[s][1] == 0]:
-                    r = running.pop(slot)[0]
-                    r.result = self.engine.result(h, slot)
-                    r.finished = self.clock() - t0
-                    self.engine.park(h, slot)
-                    free[self.slot_region[slot]].append(slot)
-                    self.log.append(("finish", r.finished, r.rid, slot))
-                    if self.on_finish is not None:
-                        self.on_finish(r)
+                for reg, _ in ks:
+                    if hasattr(self.engine, "check"):
+                        self.engine.check(reg.handle)
+                self.log.append(("turn", tt - t0, self.clock() - tt, [(reg.g, k) for reg, k in ks]))
+                for reg, k in ks:
+                    for slot in sorted(reg.running):
+                        reg.running[slot][1] -= k
+                    for slot in [sl for sl in sorted(reg.running) if reg.running[sl][1] == 0]:
+                        r = reg.running.pop(slot)[0]
+                        r.result = self.engine.result(reg.handle, slot)
+                        r.finished = self.clock() - t0
+                        self.engine.park(reg.handle, slot)
+                        reg.free.append(slot)
+                        self.log.append(("finish", r.finished, r.rid, r.region, slot))
+                        if self.on_finish is not None:
+                            self.on_finish(r)
         finally:
-            self.engine.close(h)
+            for reg in regs:
+                self.engine.close(reg.handle)
         return list(requests)
 
 
@@ -513,8 +557,7 @@ def _main_slots(a) -> int:
                           "arrival_s": round(r.arrival, 3), "admitted_s": round(r.admitted, 3),
                           "ttf_s": round(r.time_to_forecast, 3)}), file=sys.stderr, flush=True)
 
-    srv = SlotServer(SlotEngine(precision=a.precision), regions, a.slots_per_region, steps_per_turn=a.steps_per_turn,
-                     on_finish=progress)
+    srv = SlotServer(SlotEngine(precision=a.precision), regions, a.slots_per_region, on_finish=progress)
     t0 = time.perf_counter()
     srv.run(reqs)
     out = summary(reqs, time.perf_counter() - t0 - srv.setup_s)

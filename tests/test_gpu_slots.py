@@ -71,6 +71,49 @@ def test_member_admitted_mid_run_equals_its_solo_run(native, precision):
         x.close()
 
 
+def _parked_beside_active(precision):
+    """Eight storm members of ~10k nodes, the even ones parked (at rest: zero right-hand side,
+    done before their first iteration), the odd ones forced; 32-row solver tiles, so ~2,600 tiles
+    over the cooperative grid's blocks put several member boundaries inside a block."""
+    from gschism_b200.model import Model
+    cs = [cases.storm(20 + i, nmin=10000, nmax=10500, nvrt=10, dt=100.0, hours=1.0)[0] for i in range(8)]
+    m = Model(cs, precision=precision)
+    m.set_launch("JCG_TILES", 592, 32)
+    for k in range(8):
+        m.set_tau(k, np.zeros(m.shape(k, "NODE_TAU")))
+        if k % 2 == 0:
+            m.park(k, m.member_state(k))
+        else:
+            m.set_vortex(k, cases.storm_on(cs[k], 100 + k))
+    return cs, m
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_ir"])
+def test_retired_member_sharing_solver_blocks_with_an_active_one(native, precision):
+    """Parked members whose solver tiles share blocks with active members' tiles: every active
+    member's solve runs to convergence without a bounded wait running out (a block holding a
+    finished member's tiles must not wait for that member's next iteration), and gives the bits
+    of its solo run with the same tiling."""
+    from gschism_b200.model import Model
+    cs, m = _parked_beside_active(precision)
+    solo = Model([cs[1]], precision=precision)
+    solo.set_launch("JCG_TILES", 592, 32)
+    solo.set_tau(0, np.zeros(solo.shape(0, "NODE_TAU")))
+    solo.set_vortex(0, cases.storm_on(cs[1], 101))
+    for _ in range(3):
+        m.step(1)
+        solo.step(1)
+        m.sync()                                                 # GS_ERR_TIMEOUT if a wait ran out
+        for k in range(8):
+            st = m.stats(k)
+            assert st["error_flags"] == 0, k
+            assert (st["jcg_iters"] == 0) if k % 2 == 0 else (st["jcg_iters"] > 0), k
+        assert m.stats(1)["jcg_iters"] == solo.stats(0)["jcg_iters"]
+    _same(m, 1, solo)
+    m.close()
+    solo.close()
+
+
 def test_members_of_one_context_share_the_vertical_grid(native):
     from gschism_b200.model import Model
     s, _, _ = cases.storm(4, nmin=4000, nmax=4500, nvrt=10, dt=100.0, hours=1.0)
@@ -91,17 +134,21 @@ def test_member_start_rejects_bad_arguments(native):
     m.close()
 
 
-def test_slot_server_on_gpu(native):
-    """The slot server end to end on two small regions: every forecast equals its solo run."""
+@pytest.mark.parametrize("precision", ["fp64", "fp32_ir"])
+def test_slot_server_on_gpu(native, precision):
+    """The slot server end to end on two small regions, with 32-row solver tiles so that parked
+    and running slots share solver blocks: every forecast equals its solo run (same tiling)."""
     from gschism_b200.model import Model
     from gschism_b200.serve import SlotEngine, SlotServer, slot_requests
-    regions = [cases.storm(7, nmin=3000, nmax=3200, nvrt=10, dt=100.0, hours=1.0)[0],
-               cases.storm(8, nmin=5000, nmax=5200, nvrt=10, dt=100.0, hours=1.0)[0]]
-    reqs = slot_requests(5, rate=200.0, seed=4, regions=regions, hours=0.25, dt=100.0)
-    srv = SlotServer(SlotEngine(precision="fp64", fields=("ETA2", "NODE_TR")), regions, 1, steps_per_turn=3)
+    regions = [cases.storm(7, nmin=9000, nmax=9500, nvrt=10, dt=100.0, hours=1.0)[0],
+               cases.storm(8, nmin=12000, nmax=12500, nvrt=10, dt=100.0, hours=1.0)[0]]
+    reqs = slot_requests(6, rate=200.0, seed=4, regions=regions, hours=0.25, dt=100.0)
+    eng = SlotEngine(precision=precision, fields=("ETA2", "NODE_TR"), jcg_tiles=(592, 32))
+    srv = SlotServer(eng, regions, 2, steps_per_turn=3)
     srv.run(reqs)
     for r in reqs:
-        solo = Model([r.case], precision="fp64")
+        solo = Model([r.case], precision=precision)
+        solo.set_launch("JCG_TILES", 592, 32)
         solo.set_tau(0, np.zeros(solo.shape(0, "NODE_TAU")))
         solo.set_vortex(0, r.vortex)
         solo.step(r.nsteps)

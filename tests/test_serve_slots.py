@@ -29,41 +29,47 @@ def _region(n):
 
 
 class FakeSlotEngine:
-    """A context step costs 1 us per 1000 nodes of all slots (parked ones included); each slot
-    counts its own steps since admission, the way the member clock does."""
+    """One fake context per region: a context step costs 1 us per 1000 nodes of its slots (parked
+    ones included); each slot counts its own steps since admission, the way the member clock
+    does."""
 
     def __init__(self, clock):
         self.clock = clock
-        self.events = []
+        self.ctx = {}
+        self.closed = set()
 
     def build(self, slot_cases):
-        self.sizes = [c.n_nodes for c in slot_cases]
-        self.own = [None] * len(slot_cases)        # steps of the slot's current run; None = parked
-        self.owner = [None] * len(slot_cases)
-        return "ctx"
+        h = len(self.ctx)
+        self.ctx[h] = {"sizes": [c.n_nodes for c in slot_cases], "own": [None] * len(slot_cases),
+                       "owner": [None] * len(slot_cases), "steps": 0}
+        return h
 
     def admit(self, h, slot, r):
-        assert self.own[slot] is None, "admitted into a busy slot"
-        self.own[slot], self.owner[slot] = 0, r.rid
-        self.events.append(("admit", r.rid, slot, self.clock.t))
+        c = self.ctx[h]
+        assert c["own"][slot] is None, "admitted into a busy slot"
+        c["own"][slot], c["owner"][slot] = 0, r.rid
 
     def advance(self, h, k):
-        self.clock.t += 1e-6 * k * sum(self.sizes) / 1000.0
-        for s in range(len(self.own)):
-            if self.own[s] is not None:
-                self.own[s] += k
+        c = self.ctx[h]
+        self.clock.t += 1e-6 * k * sum(c["sizes"]) / 1000.0
+        c["steps"] += k
+        for sl in range(len(c["own"])):
+            if c["own"][sl] is not None:
+                c["own"][sl] += k
 
     def wait(self):
         pass
 
     def result(self, h, slot):
-        return {"rid": self.owner[slot], "steps": self.own[slot]}
+        c = self.ctx[h]
+        return {"rid": c["owner"][slot], "steps": c["own"][slot]}
 
     def park(self, h, slot):
-        self.own[slot], self.owner[slot] = None, None
+        c = self.ctx[h]
+        c["own"][slot], c["owner"][slot] = None, None
 
     def close(self, h):
-        self.closed = True
+        self.closed.add(h)
 
 
 def _reqs(spec, regions=None):
@@ -82,15 +88,15 @@ def test_slots_run_every_forecast_its_horizon():
     for r in reqs:
         assert r.result == {"rid": r.rid, "steps": r.nsteps}      # its own slot, exactly its horizon
         assert r.arrival <= r.admitted <= r.finished
-        assert srv.slot_region[r.slot] == r.region
-    assert eng.closed
+        assert r.cohort == r.region                              # a slot of its own region's context
+    assert eng.closed == set(eng.ctx)
     # region 0 has two slots: the third region-0 request waits for one to free up
     first_free = min(r.finished for r in reqs[:3] if r.region == 0)
     assert reqs[3].admitted >= first_free - 1e-12
     # region 1's second request waits for its single slot
     assert reqs[4].admitted >= reqs[1].finished - 1e-12
     # a request of another region is not held up by a full region
-    assert reqs[4].admitted < reqs[3].admitted
+    assert reqs[4].admitted <= reqs[3].admitted
     s = summary(reqs, max(r.finished for r in reqs))
     assert s["requests"] == 6 and s["ttf_p50_s"] > 0
 
@@ -105,10 +111,27 @@ def test_admission_happens_while_others_run():
     srv.run(reqs)
     assert reqs[1].admitted < reqs[0].finished
     assert reqs[1].finished < reqs[0].finished
-    # turns never step past a forecast's horizon
+    # turns never step past a forecast's horizon, nor beyond steps_per_turn
     turns = [e for e in srv.log if e[0] == "turn"]
-    assert all(k <= 4 for *_, k in turns)
-    assert sum(k for *_, k in turns) == 400
+    ks = [k for *_, gk in turns for g, k in gk]
+    assert all(1 <= k <= 4 for k in ks)
+    assert sum(ks) == 400
+
+
+def test_regions_step_separately_and_idle_regions_not_at_all():
+    """A small region's context takes more steps per turn than a large one's (about the same
+    node-steps), and a region with nothing running is not stepped."""
+    clk = Clock()
+    eng = FakeSlotEngine(clk)
+    regions = [_region(20_000), _region(800_000), _region(50_000)]
+    srv = SlotServer(eng, regions, 2, steps_per_turn=64, turn_node_steps=4_000_000, clock=clk, sleep=clk.sleep)
+    reqs = _reqs([(0.0, 0, 200), (0.0, 1, 30)], regions)
+    srv.run(reqs)
+    turns = [e for e in srv.log if e[0] == "turn"]
+    first = dict(turns[0][3])
+    assert first[0] > first[1]                    # 64 steps of the small context, 2 of the large
+    assert eng.ctx[2]["steps"] == 0               # region 2 had no request
+    assert eng.ctx[0]["steps"] == 200 and eng.ctx[1]["steps"] == 30
 
 
 def test_unknown_region_is_refused():
