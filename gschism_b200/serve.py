@@ -24,9 +24,10 @@ order), so each forecast is the same alone and in the mix.
 Reported: time-to-forecast per request (arrival to results on the host), its p50/p99, and the
 node-level-steps/s of the whole run.
 
-Slot serving (`SlotServer`, `--regions R`): for a service over a fixed set of region meshes, one
-context holds member slots on those meshes and a request joins the running launch sequence at
-the next step boundary, with its own clock on the device (gs_set_member_start); see the class.
+Slot serving (`SlotServer`, `--regions R`): for a service over a fixed set of region meshes, each
+region has one context of member slots on its mesh, and a request joins its region's running
+launch sequence at the next step boundary, with its own clock on the device
+(gs_set_member_start); see the class.
 """
 from __future__ import annotations
 
